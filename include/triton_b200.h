@@ -1,0 +1,221 @@
+/* triton_b200.h -- C ABI of the B200-native TRITON time-stepping library.
+ *
+ * One shared library (triton_b200/lib/libtriton_b200.so) exports every symbol
+ * below with C linkage: plain pointers, sizes and status codes, no C++ or
+ * framework types.  Two layers are offered:
+ *
+ *  1. Kernel entry points (tri_kernel_*): one per reference device kernel,
+ *     same arguments and meaning as the reference's Kernels:: templates over
+ *     raw device pointers (reference files src/kernels*.h, TRITON 2.1.1), plus
+ *     the stream to launch on.  A maintainer replaces each Kernels::X(...) call
+ *     in triton_simulate.h with tri_kernel_X_f64(..., stream) and keeps the
+ *     rest of the reference loop unchanged.
+ *
+ *  2. Domain entry points (tri_domain_*): the B200 path.  The library owns the
+ *     device state of one simulation domain and runs whole time steps with
+ *     fused kernels, the CFL dt reduction and the reference's dt policy on the
+ *     device, stopping at the same events the reference loop reacts to
+ *     (triton_simulate.h:54-134).  This replaces compute_local_dt,
+ *     compute_global_dt and compute_new_state (triton_simulate.h:191-346) and
+ *     the device arrays of create_device_vectors (triton_init.h:1452-1591).
+ *
+ * Grid layout (both layers, as the reference's device arrays): row-major
+ * rows x cols values INCLUDING the one-cell ghost ring, id = row*cols + col,
+ * row 0 is the northern edge.  Manning values are stored squared (n^2), the
+ * closed-boundary walls are DEM ghost values of 1e6 (triton_init.h:212-237).
+ *
+ * Errors: every call returns a tri_status; tri_last_error() gives the message
+ * of the last failure on the calling thread.  Nothing exits the process.
+ */
+#ifndef TRITON_B200_H
+#define TRITON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRI_ABI_VERSION 1
+
+typedef enum tri_status {
+  TRI_OK = 0,
+  TRI_E_INVALID = 1, /* bad argument (null pointer, size mismatch, out-of-range index) */
+  TRI_E_CUDA = 2,    /* a CUDA runtime call failed (message has the CUDA error string) */
+  TRI_E_NOMEM = 3,   /* device allocation failed or the HBM budget would be exceeded */
+  TRI_E_STATE = 4,   /* call not valid in the current state */
+  TRI_E_IO = 5,      /* file could not be read or written */
+  TRI_E_TIMEOUT = 6  /* a bounded device-side wait gave up (no GPU state was lost) */
+} tri_status;
+
+typedef enum tri_precision {
+  TRI_FP64 = 0, /* plain form: FP64 throughout, matches the reference */
+  TRI_FP32 = 1  /* precision form: FP32 state, FP64 dt reduction and volume sums */
+} tri_precision;
+
+/* Field ids follow the reference's slot ids (constants.h:82-87). */
+typedef enum tri_field {
+  TRI_FIELD_H = 0,
+  TRI_FIELD_QX = 1,
+  TRI_FIELD_QY = 2,
+  TRI_FIELD_NMAN2 = 3, /* Manning n squared */
+  TRI_FIELD_DEM = 4,
+  TRI_FIELD_MAXH = 5
+} tri_field;
+
+/* Events raised by the step that ends a tri_domain_advance call; the names
+ * are the conditions triton_simulate.h checks after every step. */
+enum {
+  TRI_EV_END = 1,   /* simtime >= sim_duration (:54)                    */
+  TRI_EV_PRINT = 2, /* simtime >= print_interval*(print_id+1) (:92)     */
+  TRI_EV_OBS = 4,   /* time_series && simtime-last_obs >= print_obs (:78) */
+  TRI_EV_LOG = 8    /* it_count % it_print == 0 (:69)                   */
+};
+
+typedef struct tri_grid_desc {
+  int32_t rows, cols;      /* padded sizes: interior + 2 ghost rows/columns */
+  double cell_size;        /* dx = dy (dem header) */
+  double courant;          /* cfg "courant" */
+  double hextra;           /* cfg "hextra" */
+  int32_t open_boundaries; /* cfg "open_boundaries" */
+  int32_t precision;       /* tri_precision */
+} tri_grid_desc;
+
+/* The loop variables of triton<T>::simulate (triton_simulate.h:41-52) plus
+ * the dt-policy inputs (compute_init_dt :163-187, cfg time_step). */
+typedef struct tri_clock {
+  double simtime;
+  double sim_duration;
+  double print_interval;
+  double print_observation;
+  double last_obs_time;
+  double init_dt;    /* dt used when every cell is dry (:217-220) */
+  double time_step;  /* fixed dt when time_increment_fixed (cfg) */
+  double average_dt; /* running dt sum, reset by the caller on TRI_EV_LOG */
+  double global_dt;  /* out: dt of the last step */
+  int32_t print_id;
+  int32_t it_count;
+  int32_t it_print;
+  int32_t time_series;
+  int32_t time_increment_fixed;
+  int32_t runoff_row;  /* index_row_runoff (triton_init.h:1299-1310) */
+  int32_t src_idx_low; /* idx_low of the hydrograph search (triton.h:79) */
+  int32_t reserved;
+} tri_clock;
+
+typedef struct tri_progress {
+  int32_t steps;  /* steps run by this call */
+  int32_t events; /* OR of TRI_EV_* raised by the last step (0: max_steps reached) */
+} tri_progress;
+
+typedef struct tri_domain tri_domain;
+
+/* ---- library ---------------------------------------------------------- */
+int tri_abi_version(void);
+const char* tri_last_error(void);
+/* Device memory one domain needs for this grid, in bytes. */
+int tri_domain_footprint(const tri_grid_desc* desc, int64_t* bytes);
+
+/* ---- domain ------------------------------------------------------------ */
+/* stream: a cudaStream_t to launch on, or NULL for a stream owned by the
+ * domain.  Replaces create_device_vectors (triton_init.h:1452-1591). */
+int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out);
+int tri_domain_destroy(tri_domain* d);
+
+/* Host <-> device copies of whole padded fields (n = rows*cols values).
+ * Host arrays are always double; an FP32 domain rounds on upload.  Uploading
+ * H, QX or QY (or DEM) invalidates the cached CFL dt. */
+int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t n);
+int tri_domain_download(tri_domain* d, int32_t field, double* host, int64_t n);
+
+/* Forcing tables, flattened as in triton_init.h.
+ *  runoff  (:1299-1357): zone id per padded cell (values in [0, nzones)),
+ *          times[nrows] in s, rates[zone*nrows + row] in m/s.
+ *  sources (:723-816):   padded cell index per source, times[nrows] in s,
+ *          flows[row*nsrc + src] in m3/s.
+ *  extbc   (:913-1055):  per boundary cell its padded index, type (0..3),
+ *          start row in var1/var2 and row count; var1/var2 concatenated
+ *          tables (type 1: hours already converted to s).
+ *  observations (:818-911): padded cell indices. */
+int tri_domain_set_runoff(tri_domain* d, int32_t nzones, int32_t nrows, const double* times, const double* rates,
+                          const int32_t* zone_of_cell, int64_t ncells);
+int tri_domain_set_sources(tri_domain* d, int32_t nsrc, const int32_t* cells, int32_t nrows, const double* times,
+                           const double* flows);
+int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, const int32_t* types,
+                         const int32_t* start, const int32_t* nrows, int32_t nvars, const double* var1,
+                         const double* var2);
+int tri_domain_set_observations(tri_domain* d, int32_t nobs, const int32_t* cells);
+
+int tri_domain_set_clock(tri_domain* d, const tri_clock* clock);
+int tri_domain_get_clock(tri_domain* d, tri_clock* clock);
+
+/* Runs up to max_steps time steps on the device and returns after the first
+ * step that raises an event (or after max_steps).  The caller reacts to the
+ * events as the reference loop does (write outputs, advance print_id /
+ * last_obs_time, reset average_dt) and writes the clock back before the next
+ * call.  Blocks until the steps have finished. */
+int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* progress);
+
+/* CFL dt of the current state (compute_dt_and_sqrt + find_min_dt, kernels.h:167-212). */
+int tri_domain_compute_dt(tri_domain* d, double* local_dt);
+/* Values at the observation cells (copy_observation_points, kernels.h:522-535);
+ * any output pointer may be NULL. */
+int tri_domain_observe(tri_domain* d, double* h, double* qx, double* qy);
+/* Sum of h over interior cells times dx^2, accumulated in FP64. */
+int tri_domain_volume(tri_domain* d, double* volume);
+int tri_domain_synchronize(tri_domain* d);
+/* Kernel timing with CUDA events on the domain's stream: when enabled,
+ * advance() records the flux/update kernel and the wet-dry/dt kernel.
+ * Reports total milliseconds and launch counts since the last reset. */
+int tri_domain_set_timing(tri_domain* d, int32_t enabled);
+int tri_domain_get_timing(tri_domain* d, double* flux_ms, int32_t* flux_launches, double* wetdry_ms,
+                          int32_t* wetdry_launches);
+
+/* ---- reference kernels (FP64, device pointers) -------------------------- */
+/* Each launches on 'stream' (cudaStream_t, NULL = default stream) and does not
+ * synchronize.  size/rows/cols as in the reference; 'stream' is added last. */
+int tri_kernel_compute_dt_and_sqrt_f64(int size, double dx, const double* qx, const double* qy, const double* h,
+                                       double* sqrth, double* dt_out, double cn, double hextra, void* stream);
+/* find_min_dt: writes the minimum into *min_out (a DEVICE double) with one
+ * kernel and no scratch memory. */
+int tri_kernel_find_min_dt_f64(int size, const double* dt, double* min_out, void* stream);
+int tri_kernel_flux_x_f64(int size, int nrows, int ncols, double dx, double dt, const double* h, const double* qx,
+                          const double* qy, const double* dem, const double* sqrth, double* rhsh0, double* rhsh1,
+                          double* rhsqx0, double* rhsqx1, double* rhsqy0, double* rhsqy1, double hextra,
+                          void* stream);
+int tri_kernel_flux_y_f64(int size, int nrows, int ncols, double dx, double dt, const double* h, const double* qx,
+                          const double* qy, const double* dem, const double* sqrth, double* rhsh0, double* rhsh1,
+                          double* rhsqx0, double* rhsqx1, double* rhsqy0, double* rhsqy1, double hextra,
+                          void* stream);
+int tri_kernel_update_cells_f64(int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy,
+                                const double* dem, const double* n, double* rhsh0, double* rhsh1, double* rhsqx0,
+                                double* rhsqx1, double* rhsqy0, double* rhsqy1, double hextra, void* stream);
+int tri_kernel_update_runoff_f64(int size, int nrows, int ncols, double dt, const int32_t* runoff_id,
+                                 int index_row_runoff, int n_rows_runoff, const double* runoff_intensity, double* h,
+                                 double* qx, double* qy, double hextra, void* stream);
+/* compute_flow: sources that share a cell are applied in source order. */
+int tri_kernel_compute_flow_f64(int size, const double* hyd_time, const double* hyd_val, double dx, double dt,
+                                double simtime, int idx_low, int idx_high, double* h, const int32_t* pos,
+                                void* stream);
+int tri_kernel_copy_info_to_exterior_boundaries_west_east_f64(int size, int nrows, int ncols, double* h, double* qx,
+                                                              double* qy, void* stream);
+int tri_kernel_copy_info_to_exterior_boundaries_north_south_f64(int size, int nrows, int ncols, double* h,
+                                                                double* qx, double* qy, int rank,
+                                                                int total_process, void* stream);
+/* compute_extbc_values: cells are applied in index order where two of them
+ * touch the same cell (corners shared by two segments). */
+int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy,
+                                        const double* dem, const double* n, const int32_t* relative_index,
+                                        const int32_t* extbctype, const int32_t* start_index,
+                                        const int32_t* nrows_vars, const double* extbcvar1, const double* extbcvar2,
+                                        double simtime, int rank, int total_process, void* stream);
+int tri_kernel_wet_dry_f64(int size, int nrows, int ncols, double dt, const double* h, double* qx, double* qy,
+                           const double* dem, double* max_h, double hextra, int mpi_tasks, void* stream);
+int tri_kernel_copy_observation_points_f64(int size, const double* arr, double* obs_arr,
+                                           const int32_t* relative_index, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRITON_B200_H */

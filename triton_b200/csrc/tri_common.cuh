@@ -1,0 +1,44 @@
+// tri_common.cuh -- constants and small device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace tri {
+
+// Physical constants and tolerances of the reference (constants.h:38-50,
+// 117-118).  SQRTG is the reference's literal, not sqrt(9.81).
+constexpr double kGravity = 9.81;
+constexpr double kSqrtG = 3.132091953;
+constexpr double kMaxValue = 1e10;  // "dry" cell dt sentinel (MAX_VALUE)
+
+template <typename T>
+__host__ __device__ constexpr T eps12();
+template <>
+__host__ __device__ constexpr double eps12<double>() { return 1e-12; }
+template <>
+__host__ __device__ constexpr float eps12<float>() { return 1e-6f; }  // single-precision build value
+
+__device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double dev_cbrt(double x) { return cbrt(x); }
+__device__ __forceinline__ float dev_cbrt(float x) { return cbrtf(x); }
+__device__ __forceinline__ double dev_fabs(double x) { return fabs(x); }
+__device__ __forceinline__ float dev_fabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double dev_fmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float dev_fmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double dev_fmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float dev_fmin(float a, float b) { return fminf(a, b); }
+
+// Order-preserving key of a non-negative double for an unsigned atomic min.
+// NaN maps to +inf so it is never the minimum (the reference's
+// "a < m ? a : m" fold never selects a NaN either).
+__device__ __forceinline__ unsigned long long dt_key(double v) {
+  return (v != v) ? 0x7FF0000000000000ull : (unsigned long long)__double_as_longlong(v);
+}
+__device__ __forceinline__ unsigned long long dt_key(float v) { return dt_key((double)v); }
+
+constexpr unsigned long long kDtKeyInf = 0x7FF0000000000000ull;
+
+}  // namespace tri

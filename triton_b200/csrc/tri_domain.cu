@@ -1,0 +1,843 @@
+// tri_domain.cu -- the domain entry points of the C ABI (include/triton_b200.h).
+//
+// A domain owns the device arrays of one simulation (the reference allocates
+// them in create_device_vectors, triton_init.h:1452-1591) and runs whole time
+// steps with the fused kernels of tri_step_kernels.cuh.  The CFL dt is reduced
+// on the device and the reference's dt policy runs there too, so the steps of
+// an advance() call need no host round trip; steps are launched in chunks
+// captured as CUDA graphs and stop at the first event the reference loop
+// reacts to (triton_simulate.h:69-134).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "tri_internal.h"
+#include "tri_step_kernels.cuh"
+
+namespace tri {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+// Conflict-free waves: item k goes one wave after the latest earlier item
+// that touches one of its cells, so items sharing a cell keep their index
+// order and all others run in parallel.
+static void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<int32_t>& order,
+                        std::vector<int32_t>& wave_start) {
+  const int n = (int)touches.size();
+  std::map<int64_t, int> last;
+  std::vector<int> wave(n, 0);
+  int nw = 0;
+  for (int k = 0; k < n; k++) {
+    int w = 0;
+    for (int64_t cidx : touches[k]) {
+      auto it = last.find(cidx);
+      if (it != last.end()) w = std::max(w, it->second + 1);
+    }
+    wave[k] = w;
+    for (int64_t cidx : touches[k]) last[cidx] = w;
+    nw = std::max(nw, w + 1);
+  }
+  order.clear();
+  wave_start.assign(1, 0);
+  for (int w = 0; w < nw; w++) {
+    for (int k = 0; k < n; k++)
+      if (wave[k] == w) order.push_back(k);
+    wave_start.push_back((int32_t)order.size());
+  }
+}
+
+}  // namespace tri
+
+using namespace tri;
+
+struct tri_domain {
+  tri_grid_desc desc{};
+  int prec = TRI_FP64;
+  size_t esize = 8;
+  int64_t ncells = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // state (ping-pong) and static fields; element type double or float
+  void* h[2] = {nullptr, nullptr};
+  void* qx[2] = {nullptr, nullptr};
+  void* qy[2] = {nullptr, nullptr};
+  void* z = nullptr;
+  void* n2 = nullptr;
+  void* maxh = nullptr;
+  double* stage = nullptr;  // FP64 staging field for FP32 uploads/downloads
+  // runoff
+  int32_t nroff = 0, roff_rows = 0;
+  int32_t* zone = nullptr;
+  void* rates = nullptr;
+  double* roff_t = nullptr;
+  // sources
+  int32_t nsrc = 0, hyg_rows = 0;
+  int32_t* src_cells = nullptr;
+  int32_t* src_order = nullptr;
+  std::vector<int32_t> src_waves;
+  double* hyg_t = nullptr;
+  void* hyg_v = nullptr;
+  // external boundary cells
+  int32_t nbc = 0;
+  int32_t *bc_cells = nullptr, *bc_types = nullptr, *bc_start = nullptr, *bc_nrows = nullptr, *bc_order = nullptr;
+  std::vector<int32_t> bc_waves;
+  void *bc_v1 = nullptr, *bc_v2 = nullptr;
+  // observations
+  int32_t nobs = 0;
+  int32_t* obs_cells = nullptr;
+  double* obs_out = nullptr;
+  double* obs_host = nullptr;
+  // clock
+  DevClock* clk = nullptr;  // device
+  DevClock* mirror = nullptr;  // pinned host mirror
+  int32_t* halt_host = nullptr;  // pinned, one per chunk slot
+  bool dt_valid = false;
+  // volume reduction scratch
+  double* vol_part = nullptr;
+  double* vol_out = nullptr;
+  int vol_blocks = 0;
+  // launch shape
+  int bw = 128, rb = 16;
+  // graphs of 'graph_steps' steps
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  bool use_graphs = true;
+  // timing: CUDA event pairs around every flux and wet-dry launch, read once
+  // the timed region is over so the stream is never stalled
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;
+  size_t tev_used = 0;
+  cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+template <typename T>
+StateBufs<T> bufs(tri_domain* d) {
+  StateBufs<T> s;
+  for (int i = 0; i < 2; i++) {
+    s.h[i] = (T*)d->h[i];
+    s.qx[i] = (T*)d->qx[i];
+    s.qy[i] = (T*)d->qy[i];
+  }
+  return s;
+}
+
+void free_dev(void*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+template <typename P>
+void free_devp(P*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void drop_graph(tri_domain* d) {
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  d->graph = nullptr;
+  d->graph_steps = 0;
+}
+
+int64_t footprint_bytes(const tri_grid_desc* g) {
+  const int64_t n = (int64_t)g->rows * g->cols;
+  const int64_t es = g->precision == TRI_FP32 ? 4 : 8;
+  // 6 state buffers + z + n2 + maxh, one FP64 staging field, runoff zone ids
+  return n * es * 9 + n * 8 + n * 4 + (1 << 20);
+}
+
+template <typename T>
+__global__ void k_from_f64(const double* __restrict__ src, T* __restrict__ dst, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (T)src[i];
+}
+template <typename T>
+__global__ void k_to_f64(const T* __restrict__ src, double* __restrict__ dst, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+
+template <typename T>
+__global__ void k_observe(const DevClock* __restrict__ clk, StateBufs<T> sb, const int32_t* __restrict__ cells,
+                          int nobs, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nobs) return;
+  const int b = clk->cur;
+  const int id = cells[k];
+  out[k] = (double)sb.h[b][id];
+  out[nobs + k] = (double)sb.qx[b][id];
+  out[2 * nobs + k] = (double)sb.qy[b][id];
+}
+
+// Interior volume: each block sums a fixed set of rows in a fixed order, then
+// one block adds the partials in block order, so the result is reproducible.
+template <typename T>
+__global__ void __launch_bounds__(256) k_volume_part(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows,
+                                                     int cols, double* __restrict__ part) {
+  const T* h = sb.h[clk->cur];
+  double acc = 0.0;
+  for (int r = 1 + blockIdx.x; r <= rows - 2; r += gridDim.x)
+    for (int c = 1 + threadIdx.x; c <= cols - 2; c += blockDim.x) acc += (double)h[(size_t)r * cols + c];
+  __shared__ double s[256];
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+__global__ void k_volume_sum(const double* __restrict__ part, int n, double scale, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double acc = 0.0;
+  for (int i = 0; i < n; i++) acc += part[i];
+  *out = acc * scale;
+}
+
+void choose_shape(tri_domain* d) {
+  // Enough strips to give every SM several blocks; narrow strips waste
+  // halo columns, short strips waste halo rows.
+  const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  d->bw = cols >= 1024 ? 128 : 64;
+  const int colblocks = (cols + d->bw - 3) / (d->bw - 2);
+  const int target = 6 * sms;
+  int rb = 32;
+  while (rb > 4 && (int64_t)colblocks * ((rows + rb - 1) / rb) < target) rb /= 2;
+  d->rb = rb;
+}
+
+template <typename T>
+int launch_step(tri_domain* d) {
+  const int rows = d->desc.rows, cols = d->desc.cols;
+  const T dx = (T)d->desc.cell_size, hx = (T)d->desc.hextra, cn = (T)d->desc.courant;
+  StateBufs<T> sb = bufs<T>(d);
+  k_clock<<<1, 32, 0, d->stream>>>(d->clk);
+  dim3 g1((cols - 2 + d->bw - 3) / (d->bw - 2), (rows - 2 + d->rb - 1) / d->rb);
+  cudaEvent_t* ev = nullptr;
+  if (d->timing) {
+    while (d->tev.size() < d->tev_used + 4) {
+      cudaEvent_t e;
+      TRI_CUDA_TRY(cudaEventCreate(&e));
+      d->tev.push_back(e);
+    }
+    ev = &d->tev[d->tev_used];
+    d->tev_used += 4;
+    cudaEventRecord(ev[0], d->stream);
+  }
+  if (d->bw == 128)
+    k_flux_update<T, 128><<<g1, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
+                                                      (const T*)d->rates, rows, cols, d->rb, dx, hx);
+  else
+    k_flux_update<T, 64><<<g1, 64, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
+                                                    (const T*)d->rates, rows, cols, d->rb, dx, hx);
+  if (ev) cudaEventRecord(ev[1], d->stream);
+  if (d->nsrc > 0) {
+    for (size_t w = 0; w + 1 < d->src_waves.size(); w++) {
+      const int off = d->src_waves[w], cnt = d->src_waves[w + 1] - off;
+      k_sources<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, d->src_order + off, cnt, d->nsrc,
+                                                             d->src_cells, d->hyg_t, (const T*)d->hyg_v, dx);
+    }
+  }
+  if (d->desc.open_boundaries) {
+    const int n = std::max(rows, cols);
+    k_open_bc<T><<<(n + 255) / 256, 256, 0, d->stream>>>(d->clk, sb, rows, cols);
+  }
+  if (d->nbc > 0) {
+    for (size_t w = 0; w + 1 < d->bc_waves.size(); w++) {
+      const int off = d->bc_waves[w], cnt = d->bc_waves[w + 1] - off;
+      k_extbc<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2,
+                                                           d->bc_order + off, cnt, d->bc_cells, d->bc_types,
+                                                           d->bc_start, d->bc_nrows, (const T*)d->bc_v1,
+                                                           (const T*)d->bc_v2, rows, cols);
+    }
+  }
+  dim3 b2(32, 8), g2((cols + 31) / 32, (rows + 7) / 8);
+  if (ev) cudaEventRecord(ev[2], d->stream);
+  k_wetdry_dt<T, true><<<g2, b2, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (T*)d->maxh, rows, cols, dx, cn, hx);
+  if (ev) cudaEventRecord(ev[3], d->stream);
+  TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
+template <typename T>
+int launch_initial_dt(tri_domain* d) {
+  const int rows = d->desc.rows, cols = d->desc.cols;
+  dim3 b2(32, 8), g2((cols + 31) / 32, (rows + 7) / 8);
+  k_wetdry_dt<T, false><<<g2, b2, 0, d->stream>>>(d->clk, bufs<T>(d), (const T*)d->z, (T*)d->maxh, rows, cols,
+                                                  (T)d->desc.cell_size, (T)d->desc.courant, (T)d->desc.hextra);
+  TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
+int launch_steps(tri_domain* d, int n) {
+  if (d->use_graphs && !d->timing) {
+    const int G = 8;
+    if (!d->graph) {
+      cudaGraph_t g = nullptr;
+      TRI_CUDA_TRY(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = TRI_OK;
+      for (int i = 0; i < G && rc == TRI_OK; i++)
+        rc = d->prec == TRI_FP64 ? launch_step<double>(d) : launch_step<float>(d);
+      cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+      if (rc != TRI_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return set_error(TRI_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&d->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return set_error(TRI_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+      d->graph_steps = G;
+    }
+    while (n >= d->graph_steps) {
+      TRI_CUDA_TRY(cudaGraphLaunch(d->graph, d->stream));
+      n -= d->graph_steps;
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    int rc = d->prec == TRI_FP64 ? launch_step<double>(d) : launch_step<float>(d);
+    if (rc != TRI_OK) return rc;
+  }
+  return TRI_OK;
+}
+
+int field_ptr(tri_domain* d, int field, void** p) {
+  switch (field) {
+    case TRI_FIELD_H: *p = d->h[d->mirror->cur]; return TRI_OK;
+    case TRI_FIELD_QX: *p = d->qx[d->mirror->cur]; return TRI_OK;
+    case TRI_FIELD_QY: *p = d->qy[d->mirror->cur]; return TRI_OK;
+    case TRI_FIELD_NMAN2: *p = d->n2; return TRI_OK;
+    case TRI_FIELD_DEM: *p = d->z; return TRI_OK;
+    case TRI_FIELD_MAXH: *p = d->maxh; return TRI_OK;
+  }
+  return set_error(TRI_E_INVALID, "unknown field id %d", field);
+}
+
+template <typename T>
+int upload_table(tri_domain* d, const double* host, int64_t n, void** dst) {
+  free_dev(*dst);
+  const int64_t m = std::max<int64_t>(n, 1);
+  TRI_CUDA_TRY(cudaMalloc(dst, m * sizeof(T)));
+  if (n == 0) return TRI_OK;
+  if (sizeof(T) == 8) {
+    TRI_CUDA_TRY(cudaMemcpyAsync(*dst, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+  } else {
+    std::vector<float> tmp(host, host + n);
+    TRI_CUDA_TRY(cudaMemcpyAsync(*dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, d->stream));
+    TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  }
+  return TRI_OK;
+}
+
+int upload_raw(tri_domain* d, const void* host, size_t bytes, void** dst) {
+  free_dev(*dst);
+  TRI_CUDA_TRY(cudaMalloc(dst, std::max<size_t>(bytes, 8)));
+  if (bytes) TRI_CUDA_TRY(cudaMemcpyAsync(*dst, host, bytes, cudaMemcpyHostToDevice, d->stream));
+  return TRI_OK;
+}
+
+int push_clock(tri_domain* d) {
+  TRI_CUDA_TRY(cudaMemcpyAsync(d->clk, d->mirror, sizeof(DevClock), cudaMemcpyHostToDevice, d->stream));
+  return TRI_OK;
+}
+int pull_clock(tri_domain* d) {
+  TRI_CUDA_TRY(cudaMemcpyAsync(d->mirror, d->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, d->stream));
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tri_abi_version(void) { return TRI_ABI_VERSION; }
+
+const char* tri_last_error(void) { return g_last_error.c_str(); }
+
+int tri_domain_footprint(const tri_grid_desc* desc, int64_t* bytes) {
+  TRI_CHECK_ARG(desc && bytes, "null argument");
+  *bytes = footprint_bytes(desc);
+  return TRI_OK;
+}
+
+int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out) {
+  TRI_CHECK_ARG(desc && out, "null argument");
+  TRI_CHECK_ARG(desc->rows >= 3 && desc->cols >= 3, "grid must have at least one interior cell (rows=%d cols=%d)",
+                desc->rows, desc->cols);
+  TRI_CHECK_ARG((int64_t)desc->rows * desc->cols < (int64_t)1 << 31, "grid too large for 32-bit cell indices");
+  TRI_CHECK_ARG(desc->cell_size > 0, "cell_size must be positive");
+  TRI_CHECK_ARG(desc->precision == TRI_FP64 || desc->precision == TRI_FP32, "unknown precision %d", desc->precision);
+  *out = nullptr;
+  tri_domain* d = new tri_domain();
+  d->desc = *desc;
+  d->prec = desc->precision;
+  d->esize = d->prec == TRI_FP64 ? 8 : 4;
+  d->ncells = (int64_t)desc->rows * desc->cols;
+  int rc = TRI_OK;
+  auto fail = [&](int code) {
+    tri_domain_destroy(d);
+    return code;
+  };
+  if (stream) {
+    d->stream = as_stream(stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(set_error(TRI_E_CUDA, "cannot create a CUDA stream (is a GPU visible?)"));
+    d->own_stream = true;
+  }
+  const size_t fb = d->ncells * d->esize;
+  void** fields[] = {&d->h[0], &d->h[1], &d->qx[0], &d->qx[1], &d->qy[0], &d->qy[1], &d->z, &d->n2, &d->maxh};
+  for (void** f : fields) {
+    cudaError_t e = cudaMalloc(f, fb);
+    if (e != cudaSuccess)
+      return fail(set_error(e == cudaErrorMemoryAllocation ? TRI_E_NOMEM : TRI_E_CUDA, "cudaMalloc(%zu): %s", fb,
+                            cudaGetErrorString(e)));
+    cudaMemsetAsync(*f, 0, fb, d->stream);
+  }
+  if (d->prec == TRI_FP32) {
+    if (cudaMalloc((void**)&d->stage, d->ncells * 8) != cudaSuccess)
+      return fail(set_error(TRI_E_NOMEM, "cudaMalloc staging field failed"));
+  }
+  if (cudaMalloc((void**)&d->clk, sizeof(DevClock)) != cudaSuccess ||
+      cudaMallocHost((void**)&d->mirror, sizeof(DevClock)) != cudaSuccess ||
+      cudaMallocHost((void**)&d->halt_host, 2 * sizeof(int32_t)) != cudaSuccess)
+    return fail(set_error(TRI_E_CUDA, "clock allocation failed"));
+  memset(d->mirror, 0, sizeof(DevClock));
+  d->mirror->dt_key[0] = d->mirror->dt_key[1] = kDtKeyInf;
+  d->mirror->sim_duration = 0;
+  d->mirror->print_interval = 1e300;
+  d->mirror->print_observation = 1e300;
+  d->mirror->init_dt = 0.01;
+  d->vol_blocks = 296;
+  if (cudaMalloc((void**)&d->vol_part, d->vol_blocks * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&d->vol_out, sizeof(double)) != cudaSuccess)
+    return fail(set_error(TRI_E_CUDA, "volume scratch allocation failed"));
+  for (int i = 0; i < 2; i++) cudaEventCreateWithFlags(&d->chunk_ev[i], cudaEventDisableTiming);
+  choose_shape(d);
+  rc = push_clock(d);
+  if (rc != TRI_OK) return fail(rc);
+  cudaError_t e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return fail(set_error(TRI_E_CUDA, "domain init: %s", cudaGetErrorString(e)));
+  *out = d;
+  return TRI_OK;
+}
+
+int tri_domain_destroy(tri_domain* d) {
+  if (!d) return TRI_OK;
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  drop_graph(d);
+  for (int i = 0; i < 2; i++) {
+    free_dev(d->h[i]);
+    free_dev(d->qx[i]);
+    free_dev(d->qy[i]);
+  }
+  free_dev(d->z);
+  free_dev(d->n2);
+  free_dev(d->maxh);
+  free_devp(d->stage);
+  free_devp(d->zone);
+  free_dev(d->rates);
+  free_devp(d->roff_t);
+  free_devp(d->src_cells);
+  free_devp(d->src_order);
+  free_devp(d->hyg_t);
+  free_dev(d->hyg_v);
+  free_devp(d->bc_cells);
+  free_devp(d->bc_types);
+  free_devp(d->bc_start);
+  free_devp(d->bc_nrows);
+  free_devp(d->bc_order);
+  free_dev(d->bc_v1);
+  free_dev(d->bc_v2);
+  free_devp(d->obs_cells);
+  free_devp(d->obs_out);
+  free_devp(d->vol_part);
+  free_devp(d->vol_out);
+  free_devp(d->clk);
+  if (d->obs_host) cudaFreeHost(d->obs_host);
+  if (d->mirror) cudaFreeHost(d->mirror);
+  if (d->halt_host) cudaFreeHost(d->halt_host);
+  for (cudaEvent_t e : d->tev) cudaEventDestroy(e);
+  for (int i = 0; i < 2; i++)
+    if (d->chunk_ev[i]) cudaEventDestroy(d->chunk_ev[i]);
+  if (d->own_stream && d->stream) cudaStreamDestroy(d->stream);
+  delete d;
+  return TRI_OK;
+}
+
+int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t n) {
+  TRI_CHECK_ARG(d && host, "null argument");
+  TRI_CHECK_ARG(n == d->ncells, "field size %lld != rows*cols %lld", (long long)n, (long long)d->ncells);
+  void* p = nullptr;
+  int rc = field_ptr(d, field, &p);
+  if (rc != TRI_OK) return rc;
+  if (d->prec == TRI_FP64) {
+    TRI_CUDA_TRY(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+  } else {
+    TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+    k_from_f64<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, (float*)p, n);
+    TRI_CUDA_TRY(cudaGetLastError());
+  }
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (field != TRI_FIELD_MAXH && field != TRI_FIELD_NMAN2) d->dt_valid = false;
+  return TRI_OK;
+}
+
+int tri_domain_download(tri_domain* d, int32_t field, double* host, int64_t n) {
+  TRI_CHECK_ARG(d && host, "null argument");
+  TRI_CHECK_ARG(n == d->ncells, "field size %lld != rows*cols %lld", (long long)n, (long long)d->ncells);
+  void* p = nullptr;
+  int rc = field_ptr(d, field, &p);
+  if (rc != TRI_OK) return rc;
+  if (d->prec == TRI_FP64) {
+    TRI_CUDA_TRY(cudaMemcpyAsync(host, p, n * 8, cudaMemcpyDeviceToHost, d->stream));
+  } else {
+    k_to_f64<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const float*)p, d->stage, n);
+    TRI_CUDA_TRY(cudaGetLastError());
+    TRI_CUDA_TRY(cudaMemcpyAsync(host, d->stage, n * 8, cudaMemcpyDeviceToHost, d->stream));
+  }
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+int tri_domain_set_runoff(tri_domain* d, int32_t nzones, int32_t nrows, const double* times, const double* rates,
+                          const int32_t* zone_of_cell, int64_t ncells) {
+  TRI_CHECK_ARG(d, "null domain");
+  drop_graph(d);
+  if (nzones <= 0) {
+    d->nroff = 0;
+    d->mirror->nroff = 0;
+    return TRI_OK;
+  }
+  TRI_CHECK_ARG(times && rates && zone_of_cell, "null runoff table");
+  TRI_CHECK_ARG(nrows >= 2, "runoff table needs at least two rows (got %d)", nrows);
+  TRI_CHECK_ARG(ncells == d->ncells, "runoff map size %lld != rows*cols", (long long)ncells);
+  const int R = d->desc.rows, Cc = d->desc.cols;
+  for (int r = 1; r <= R - 2; r++)
+    for (int c = 1; c <= Cc - 2; c++) {
+      const int32_t zid = zone_of_cell[(size_t)r * Cc + c];
+      TRI_CHECK_ARG(zid >= 0 && zid < nzones, "runoff zone %d at cell (%d,%d) outside [0,%d)", zid, r, c, nzones);
+    }
+  int rc;
+  if ((rc = upload_raw(d, zone_of_cell, ncells * 4, (void**)&d->zone)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, times, nrows * 8, (void**)&d->roff_t)) != TRI_OK) return rc;
+  rc = d->prec == TRI_FP64 ? upload_table<double>(d, rates, (int64_t)nzones * nrows, &d->rates)
+                           : upload_table<float>(d, rates, (int64_t)nzones * nrows, &d->rates);
+  if (rc != TRI_OK) return rc;
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->nroff = nzones;
+  d->roff_rows = nrows;
+  d->mirror->nroff = nzones;
+  d->mirror->roff_rows = nrows;
+  d->mirror->roff_t = d->roff_t;
+  return TRI_OK;
+}
+
+int tri_domain_set_sources(tri_domain* d, int32_t nsrc, const int32_t* cells, int32_t nrows, const double* times,
+                           const double* flows) {
+  TRI_CHECK_ARG(d, "null domain");
+  drop_graph(d);
+  if (nsrc <= 0) {
+    d->nsrc = 0;
+    d->mirror->nsrc = 0;
+    return TRI_OK;
+  }
+  TRI_CHECK_ARG(cells && times && flows, "null source table");
+  TRI_CHECK_ARG(nrows >= 2, "hydrograph needs at least two rows (got %d)", nrows);
+  const int R = d->desc.rows, Cc = d->desc.cols;
+  std::vector<std::vector<int64_t>> touch(nsrc);
+  for (int i = 0; i < nsrc; i++) {
+    const int r = cells[i] / Cc, c = cells[i] % Cc;
+    TRI_CHECK_ARG(cells[i] >= 0 && r >= 1 && r <= R - 2 && c >= 1 && c <= Cc - 2,
+                  "source %d cell index %d is not an interior cell", i + 1, cells[i]);
+    touch[i].push_back(cells[i]);
+  }
+  std::vector<int32_t> order;
+  build_waves(touch, order, d->src_waves);
+  int rc;
+  if ((rc = upload_raw(d, cells, nsrc * 4, (void**)&d->src_cells)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, order.data(), order.size() * 4, (void**)&d->src_order)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, times, nrows * 8, (void**)&d->hyg_t)) != TRI_OK) return rc;
+  rc = d->prec == TRI_FP64 ? upload_table<double>(d, flows, (int64_t)nsrc * nrows, &d->hyg_v)
+                           : upload_table<float>(d, flows, (int64_t)nsrc * nrows, &d->hyg_v);
+  if (rc != TRI_OK) return rc;
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->nsrc = nsrc;
+  d->hyg_rows = nrows;
+  d->mirror->nsrc = nsrc;
+  d->mirror->hyg_rows = nrows;
+  d->mirror->hyg_t = d->hyg_t;
+  return TRI_OK;
+}
+
+int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, const int32_t* types,
+                         const int32_t* start, const int32_t* nrows, int32_t nvars, const double* var1,
+                         const double* var2) {
+  TRI_CHECK_ARG(d, "null domain");
+  drop_graph(d);
+  if (ncells <= 0) {
+    d->nbc = 0;
+    return TRI_OK;
+  }
+  TRI_CHECK_ARG(cells && types && start && nrows && var1 && var2, "null extbc table");
+  const int R = d->desc.rows, Cc = d->desc.cols;
+  std::vector<std::vector<int64_t>> touch(ncells);
+  for (int i = 0; i < ncells; i++) {
+    const int ii = cells[i];
+    TRI_CHECK_ARG(ii >= 0 && ii < R * Cc, "extbc cell %d index %d outside the grid", i, ii);
+    TRI_CHECK_ARG(types[i] >= 0 && types[i] <= 3, "extbc cell %d has unknown type %d", i, types[i]);
+    TRI_CHECK_ARG(nrows[i] >= 1 && start[i] >= 0 && start[i] + nrows[i] <= nvars,
+                  "extbc cell %d table rows [%d,%d) outside [0,%d)", i, start[i], start[i] + nrows[i], nvars);
+    const int ix = ii / Cc, iy = ii % Cc;
+    TRI_CHECK_ARG(ix >= 1 && ix <= R - 2 && iy >= 1 && iy <= Cc - 2, "extbc cell %d is not an interior cell", i);
+    // the inner cell, the ghost it writes and, at a corner, the second ghost
+    touch[i] = {ii, (int64_t)ii - 1, (int64_t)ii + 1, (int64_t)ii - Cc, (int64_t)ii + Cc};
+  }
+  std::vector<int32_t> order;
+  build_waves(touch, order, d->bc_waves);
+  int rc;
+  if ((rc = upload_raw(d, cells, ncells * 4, (void**)&d->bc_cells)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, types, ncells * 4, (void**)&d->bc_types)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, start, ncells * 4, (void**)&d->bc_start)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, nrows, ncells * 4, (void**)&d->bc_nrows)) != TRI_OK) return rc;
+  if ((rc = upload_raw(d, order.data(), order.size() * 4, (void**)&d->bc_order)) != TRI_OK) return rc;
+  rc = d->prec == TRI_FP64 ? upload_table<double>(d, var1, nvars, &d->bc_v1) : upload_table<float>(d, var1, nvars, &d->bc_v1);
+  if (rc != TRI_OK) return rc;
+  rc = d->prec == TRI_FP64 ? upload_table<double>(d, var2, nvars, &d->bc_v2) : upload_table<float>(d, var2, nvars, &d->bc_v2);
+  if (rc != TRI_OK) return rc;
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->nbc = ncells;
+  return TRI_OK;
+}
+
+int tri_domain_set_observations(tri_domain* d, int32_t nobs, const int32_t* cells) {
+  TRI_CHECK_ARG(d, "null domain");
+  free_devp(d->obs_cells);
+  free_devp(d->obs_out);
+  if (d->obs_host) cudaFreeHost(d->obs_host);
+  d->obs_host = nullptr;
+  d->nobs = 0;
+  if (nobs <= 0) return TRI_OK;
+  TRI_CHECK_ARG(cells, "null observation cells");
+  for (int i = 0; i < nobs; i++)
+    TRI_CHECK_ARG(cells[i] >= 0 && cells[i] < d->ncells, "observation %d cell index %d outside the grid", i + 1,
+                  cells[i]);
+  int rc = upload_raw(d, cells, nobs * 4, (void**)&d->obs_cells);
+  if (rc != TRI_OK) return rc;
+  TRI_CUDA_TRY(cudaMalloc((void**)&d->obs_out, 3 * nobs * sizeof(double)));
+  TRI_CUDA_TRY(cudaMallocHost((void**)&d->obs_host, 3 * nobs * sizeof(double)));
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->nobs = nobs;
+  return TRI_OK;
+}
+
+int tri_domain_set_clock(tri_domain* d, const tri_clock* c) {
+  TRI_CHECK_ARG(d && c, "null argument");
+  DevClock* m = d->mirror;
+  m->simtime = c->simtime;
+  m->sim_duration = c->sim_duration;
+  m->print_interval = c->print_interval;
+  m->print_observation = c->print_observation;
+  m->last_obs_time = c->last_obs_time;
+  m->init_dt = c->init_dt;
+  m->time_step = c->time_step;
+  m->average_dt = c->average_dt;
+  m->global_dt = c->global_dt;
+  m->print_id = c->print_id;
+  m->it_count = c->it_count;
+  m->it_print = c->it_print;
+  m->time_series = c->time_series;
+  m->time_increment_fixed = c->time_increment_fixed;
+  m->runoff_row = c->runoff_row;
+  m->src_idx_low = c->src_idx_low;
+  return TRI_OK;
+}
+
+int tri_domain_get_clock(tri_domain* d, tri_clock* c) {
+  TRI_CHECK_ARG(d && c, "null argument");
+  const DevClock* m = d->mirror;
+  c->simtime = m->simtime;
+  c->sim_duration = m->sim_duration;
+  c->print_interval = m->print_interval;
+  c->print_observation = m->print_observation;
+  c->last_obs_time = m->last_obs_time;
+  c->init_dt = m->init_dt;
+  c->time_step = m->time_step;
+  c->average_dt = m->average_dt;
+  c->global_dt = m->global_dt;
+  c->print_id = m->print_id;
+  c->it_count = m->it_count;
+  c->it_print = m->it_print;
+  c->time_series = m->time_series;
+  c->time_increment_fixed = m->time_increment_fixed;
+  c->runoff_row = m->runoff_row;
+  c->src_idx_low = m->src_idx_low;
+  c->reserved = 0;
+  return TRI_OK;
+}
+
+int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* p) {
+  TRI_CHECK_ARG(d && p, "null argument");
+  TRI_CHECK_ARG(max_steps >= 0, "max_steps must be >= 0");
+  p->steps = 0;
+  p->events = 0;
+  DevClock* m = d->mirror;
+  if (!(m->simtime < m->sim_duration)) {
+    p->events = TRI_EV_END;
+    return TRI_OK;
+  }
+  if (max_steps == 0) return TRI_OK;
+  TRI_CHECK_ARG(d->nroff == 0 || (m->runoff_row >= 0 && m->runoff_row < d->roff_rows),
+                "runoff_row %d outside the runoff table [0,%d)", m->runoff_row, d->roff_rows);
+  TRI_CHECK_ARG(d->nsrc == 0 || (m->src_idx_low >= 0 && m->src_idx_low < d->hyg_rows),
+                "src_idx_low %d outside the hydrograph [0,%d)", m->src_idx_low, d->hyg_rows);
+  TRI_CHECK_ARG(m->print_interval > 0, "print_interval must be positive");
+  m->halt = 0;
+  m->events = 0;
+  m->steps = 0;
+  m->status = 0;
+  const bool need_dt = !d->dt_valid && !m->time_increment_fixed;
+  if (need_dt) m->dt_key[m->rd] = kDtKeyInf;
+  int rc = push_clock(d);
+  if (rc != TRI_OK) return rc;
+  if (need_dt) {
+    rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+    if (rc != TRI_OK) return rc;
+  }
+  d->dt_valid = true;
+  // Chunks of steps, two in flight: after launching chunk k the host waits
+  // for chunk k-1 and stops launching once a step has raised an event.
+  const int chunk = 8;
+  int left = max_steps, k = 0;
+  bool halted = false;
+  while (left > 0 && !halted) {
+    const int n = std::min(chunk, left);
+    rc = launch_steps(d, n);
+    if (rc != TRI_OK) return rc;
+    TRI_CUDA_TRY(cudaMemcpyAsync(&d->halt_host[k & 1], &d->clk->halt, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 d->stream));
+    TRI_CUDA_TRY(cudaEventRecord(d->chunk_ev[k & 1], d->stream));
+    left -= n;
+    if (k > 0) {
+      TRI_CUDA_TRY(cudaEventSynchronize(d->chunk_ev[(k - 1) & 1]));
+      if (d->halt_host[(k - 1) & 1]) halted = true;
+    }
+    k++;
+  }
+  rc = pull_clock(d);
+  if (rc != TRI_OK) return rc;
+  p->steps = m->steps;
+  p->events = m->events;
+  return TRI_OK;
+}
+
+int tri_domain_compute_dt(tri_domain* d, double* local_dt) {
+  TRI_CHECK_ARG(d && local_dt, "null argument");
+  DevClock* m = d->mirror;
+  m->dt_key[m->rd] = kDtKeyInf;
+  int rc = push_clock(d);
+  if (rc != TRI_OK) return rc;
+  rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+  if (rc != TRI_OK) return rc;
+  rc = pull_clock(d);
+  if (rc != TRI_OK) return rc;
+  d->dt_valid = true;
+  const unsigned long long key = m->dt_key[m->rd];
+  double v;
+  if (key >= kDtKeyInf) {
+    v = 1.7976931348623157e308;
+  } else {
+    memcpy(&v, &key, 8);
+  }
+  *local_dt = v;
+  return TRI_OK;
+}
+
+int tri_domain_observe(tri_domain* d, double* h, double* qx, double* qy) {
+  TRI_CHECK_ARG(d, "null domain");
+  if (d->nobs == 0) return TRI_OK;
+  if (d->prec == TRI_FP64)
+    k_observe<double><<<(d->nobs + 127) / 128, 128, 0, d->stream>>>(d->clk, bufs<double>(d), d->obs_cells, d->nobs,
+                                                                     d->obs_out);
+  else
+    k_observe<float><<<(d->nobs + 127) / 128, 128, 0, d->stream>>>(d->clk, bufs<float>(d), d->obs_cells, d->nobs,
+                                                                   d->obs_out);
+  TRI_CUDA_TRY(cudaGetLastError());
+  TRI_CUDA_TRY(cudaMemcpyAsync(d->obs_host, d->obs_out, 3 * d->nobs * sizeof(double), cudaMemcpyDeviceToHost,
+                               d->stream));
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (h) memcpy(h, d->obs_host, d->nobs * sizeof(double));
+  if (qx) memcpy(qx, d->obs_host + d->nobs, d->nobs * sizeof(double));
+  if (qy) memcpy(qy, d->obs_host + 2 * d->nobs, d->nobs * sizeof(double));
+  return TRI_OK;
+}
+
+int tri_domain_volume(tri_domain* d, double* volume) {
+  TRI_CHECK_ARG(d && volume, "null argument");
+  const double dx = d->desc.cell_size;
+  if (d->prec == TRI_FP64)
+    k_volume_part<double><<<d->vol_blocks, 256, 0, d->stream>>>(d->clk, bufs<double>(d), d->desc.rows, d->desc.cols,
+                                                                d->vol_part);
+  else
+    k_volume_part<float><<<d->vol_blocks, 256, 0, d->stream>>>(d->clk, bufs<float>(d), d->desc.rows, d->desc.cols,
+                                                               d->vol_part);
+  k_volume_sum<<<1, 32, 0, d->stream>>>(d->vol_part, d->vol_blocks, dx * dx, d->vol_out);
+  TRI_CUDA_TRY(cudaGetLastError());
+  TRI_CUDA_TRY(cudaMemcpyAsync(volume, d->vol_out, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+int tri_domain_synchronize(tri_domain* d) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+int tri_domain_set_timing(tri_domain* d, int32_t enabled) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->timing = enabled != 0;
+  d->tev_used = 0;
+  return TRI_OK;
+}
+
+int tri_domain_get_timing(tri_domain* d, double* flux_ms, int32_t* flux_launches, double* wetdry_ms,
+                          int32_t* wetdry_launches) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  double fa = 0, wa = 0;
+  for (size_t i = 0; i + 3 < d->tev_used; i += 4) {
+    float a = 0, b = 0;
+    TRI_CUDA_TRY(cudaEventElapsedTime(&a, d->tev[i], d->tev[i + 1]));
+    TRI_CUDA_TRY(cudaEventElapsedTime(&b, d->tev[i + 2], d->tev[i + 3]));
+    fa += a;
+    wa += b;
+  }
+  if (flux_ms) *flux_ms = fa;
+  if (flux_launches) *flux_launches = (int32_t)(d->tev_used / 4);
+  if (wetdry_ms) *wetdry_ms = wa;
+  if (wetdry_launches) *wetdry_launches = (int32_t)(d->tev_used / 4);
+  return TRI_OK;
+}
+
+}  // extern "C"

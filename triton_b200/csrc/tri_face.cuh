@@ -1,0 +1,224 @@
+// tri_face.cuh -- the per-face augmented Roe solver of TRITON, as a device
+// function shared by every step kernel in this library.
+//
+// Reference: kernels_flux.h:84-273 (x faces, normal (1,0)) and :367-556
+// (y faces, normal (0,1)).  "1" is the cell that owns the face, "2" the
+// neighbour across it (east for x faces, NORTH for y faces: row-1).
+//
+// Bit-exactness contract: with T=double and the library's compile flags
+// (--fmad=false, IEEE div/sqrt), the value of every expression below equals
+// the reference's, because each expression keeps the reference's operand
+// order and association.  The normal components are compile-time constants;
+// the multiplications by them are kept (x*0.0 is not x in IEEE arithmetic).
+#pragma once
+
+#include "tri_common.cuh"
+
+namespace tri {
+
+// Cell quantities every face of a cell uses, computed once per cell:
+// velocities are zero below hextra (kernels_flux.h:98-117) and sqrt(h) is the
+// reference's SQRTH array (kernels.h:178).
+template <typename T>
+struct CellQ {
+  T h, qx, qy, z, sq, u, v;
+};
+
+template <typename T>
+__device__ __forceinline__ CellQ<T> make_cell(T h, T qx, T qy, T z, T hextra) {
+  CellQ<T> c;
+  c.h = h;
+  c.qx = qx;
+  c.qy = qy;
+  c.z = z;
+  c.sq = dev_fmax(dev_sqrt(h), T(0));
+  if (h >= hextra) {
+    c.u = qx / h;
+    c.v = qy / h;
+  } else {
+    c.u = T(0);
+    c.v = T(0);
+  }
+  return c;
+}
+
+// Result of one face: contributions to the owner (a) and to the neighbour (b),
+// already scaled as rhs = dt*d/dx (kernels_flux.h:267-273).  'wet' is false for
+// a dry-dry face (both scaled triples are then +0).
+template <typename T>
+struct FaceOut {
+  T a0, a1, a2, b0, b1, b2;
+};
+
+template <typename T, bool XFACE>
+__device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<T>& c2, T dx, T dt, T hextra) {
+  constexpr T nx = XFACE ? T(1) : T(0);
+  constexpr T ny = XFACE ? T(0) : T(1);
+  const T G = T(kGravity), SG = T(kSqrtG), E12 = eps12<T>();
+  FaceOut<T> out;
+  out.a0 = out.a1 = out.a2 = out.b0 = out.b1 = out.b2 = T(0);
+
+  const T h1 = c1.h, h2 = c2.h;
+  if (!(h1 > T(0) || h2 > T(0))) return out;
+
+  const T u1 = c1.u, v1 = c1.v, u2 = c2.u, v2 = c2.v;
+  const T sqh1 = c1.sq, sqh2 = c2.sq;
+
+  // Roe-averaged state and wave speeds
+  const T h12 = T(0.5) * (h1 + h2);
+  const T dh = h2 - h1;
+  const T c12 = dev_sqrt(G * h12);
+  const T u12 = (u1 * sqh1 + u2 * sqh2) / (sqh1 + sqh2);
+  const T v12 = (v1 * sqh1 + v2 * sqh2) / (sqh1 + sqh2);
+  const T un = u12 * nx + v12 * ny;
+  T lam0 = un - c12, lam1 = un, lam2 = un + c12;
+  T lamE0 = T(0), lamE2 = T(0);  // lamE1 is always zero
+
+  // Harten-Hyman style entropy fix on the acoustic waves
+  {
+    T e1 = u1 * nx + v1 * ny - SG * sqh1;
+    T e2 = u2 * nx + v2 * ny - SG * sqh2;
+    if (e1 < T(0) && e2 > T(0)) {
+      lamE0 = lam0 - e1 * (e2 - lam0) / (e2 - e1);
+      lam0 = e1 * (e2 - lam0) / (e2 - e1);
+    }
+    e1 = u1 * nx + v1 * ny + SG * sqh1;
+    e2 = u2 * nx + v2 * ny + SG * sqh2;
+    if (e1 < T(0) && e2 > T(0)) {
+      lamE2 = lam2 - e2 * (lam2 - e1) / (e2 - e1);
+      lam2 = e2 * (lam2 - e1) / (e2 - e1);
+    }
+  }
+
+  // eigenvector components (row 0 and row 2 have a leading 1, row 1 a 0)
+  const T r01 = u12 - c12 * nx, r02 = v12 - c12 * ny;
+  const T r11 = -c12 * ny, r12 = c12 * nx;
+  const T r21 = u12 + c12 * nx, r22 = v12 + c12 * ny;
+
+  // wave strengths
+  const T dqx = c2.qx - c1.qx, dqy = c2.qy - c1.qy;
+  const T al0 = T(0.5) * (dh - ((dqx * nx + dqy * ny) - un * dh) / c12);
+  const T al1 = ((dqy - v12 * dh) * nx - (dqx - u12 * dh) * ny) / c12;
+  const T al2 = T(0.5) * (dh + ((dqx * nx + dqy * ny) - un * dh) / c12);
+
+  // upwinded bed-step source, limited where the step is higher than the water
+  const T z1 = c1.z, z2 = c2.z;
+  const T dz = z2 - z1;
+  T dzp = dz, hp;
+  if (dz >= T(0)) {
+    hp = h1;
+    if (z1 + h1 < z2) dzp = h1;
+  } else {
+    hp = h2;
+    if (z2 + h2 < z1) dzp = -h2;
+  }
+  T be0 = T(0.5) * G * (hp - T(0.5) * dev_fabs(dzp)) * dzp / c12;
+
+  // positivity limiter on subcritical wet-wet faces
+  hp = h1 + al0;
+  if (lam0 * lam2 < T(0) && hp > T(0) && h1 > T(0) && h2 > T(0)) {
+    be0 = dev_fmax(be0, lam0 / (lam0 + lamE2) * (al0 * lam0 - h1 * dx * T(0.5) / dt + lamE2 * h2));
+    be0 = dev_fmin(be0, lam2 / (lam2 + lamE0) * (-al2 * lam2 + h2 * dx * T(0.5) / dt + lamE0 * h1));
+  }
+  const T be2 = -be0;
+  const T be1 = T(0);
+
+  // intermediate states decide whether mass is redirected from a dry side
+  const T l1 = hp - be0 / lam0;
+  const T l2 = hp + be2 / lam2;
+
+  T p0 = T(0), p1 = T(0), p2 = T(0);  // owner side
+  T q0 = T(0), q1 = T(0), q2 = T(0);  // neighbour side
+  if (l2 < -E12 && h2 < E12) {
+    p0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
+  } else if (l1 < -E12 && h1 < E12) {
+    q0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
+  } else {
+    // wave 0: eigenvector (1, r01, r02)
+    {
+      const T w = lam0 * al0 - be0;
+      if (lam0 > T(0)) {
+        q0 += w * T(1);
+        q1 += w * r01;
+        q2 += w * r02;
+      } else {
+        p0 += w * T(1);
+        p1 += w * r01;
+        p2 += w * r02;
+      }
+    }
+    // wave 1: eigenvector (0, r11, r12)
+    {
+      const T w = lam1 * al1 - be1;
+      if (lam1 > T(0)) {
+        q0 += w * T(0);
+        q1 += w * r11;
+        q2 += w * r12;
+      } else {
+        p0 += w * T(0);
+        p1 += w * r11;
+        p2 += w * r12;
+      }
+    }
+    // wave 2: eigenvector (1, r21, r22)
+    {
+      const T w = lam2 * al2 - be2;
+      if (lam2 > T(0)) {
+        q0 += w * T(1);
+        q1 += w * r21;
+        q2 += w * r22;
+      } else {
+        p0 += w * T(1);
+        p1 += w * r21;
+        p2 += w * r22;
+      }
+    }
+  }
+  // entropy-fix parts (lamE1 == 0 goes to the owner side, as in the reference)
+  {
+    const T w = lamE0 * al0;
+    if (lamE0 > T(0)) {
+      q0 += w * T(1);
+      q1 += w * r01;
+      q2 += w * r02;
+    } else {
+      p0 += w * T(1);
+      p1 += w * r01;
+      p2 += w * r02;
+    }
+  }
+  {
+    const T w = T(0) * al1;
+    p0 += w * T(0);
+    p1 += w * r11;
+    p2 += w * r12;
+  }
+  {
+    const T w = lamE2 * al2;
+    if (lamE2 > T(0)) {
+      q0 += w * T(1);
+      q1 += w * r21;
+      q2 += w * r22;
+    } else {
+      p0 += w * T(1);
+      p1 += w * r21;
+      p2 += w * r22;
+    }
+  }
+  // flush tiny contributions, then scale to depth/discharge increments
+  if (dev_fabs(p0) < E12) p0 = T(0);
+  if (dev_fabs(q0) < E12) q0 = T(0);
+  if (dev_fabs(p1) < E12) p1 = T(0);
+  if (dev_fabs(q1) < E12) q1 = T(0);
+  if (dev_fabs(p2) < E12) p2 = T(0);
+  if (dev_fabs(q2) < E12) q2 = T(0);
+  out.a0 = dt * p0 / dx;
+  out.a1 = dt * p1 / dx;
+  out.a2 = dt * p2 / dx;
+  out.b0 = dt * q0 / dx;
+  out.b1 = dt * q1 / dx;
+  out.b2 = dt * q2 / dx;
+  return out;
+}
+
+}  // namespace tri

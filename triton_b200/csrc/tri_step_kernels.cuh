@@ -1,0 +1,547 @@
+// tri_step_kernels.cuh -- the fused time-step kernels of the domain path.
+//
+// One time step of the reference (triton_simulate.h:191-346) becomes, on the
+// domain's stream:
+//   k_clock         1 thread: dt policy (compute_global_dt :202-226), runoff
+//                   row and hydrograph bracket (:246-285), step events
+//   k_flux_update   fluxes + conserved update + Manning friction + runoff
+//                   (kernels_flux.h, kernels_state.h, kernels.h:103-152)
+//   k_sources       point inflows (kernels.h:51-84), only with sources
+//   k_open_bc       open-boundary ghosts (kernels.h:437-512), only if open
+//   k_extbc         external boundary cells (kernels.h:237-424), only with extbc
+//   k_wetdry_dt     wet/dry masks + max depth (kernels_wetdry.h:25-93) fused
+//                   with the NEXT step's CFL dt and its min reduction
+//                   (kernels.h:167-212)
+// Every kernel reads the step's parameters from the device clock, so a
+// sequence of steps needs no host round trip and can be captured in a graph.
+#pragma once
+
+#include "tri_common.cuh"
+#include "tri_face.cuh"
+
+namespace tri {
+
+// Device-resident loop state.  Host mirror: tri_clock plus the bookkeeping
+// fields below.
+struct DevClock {
+  double simtime, sim_duration, print_interval, print_observation, last_obs_time;
+  double init_dt, time_step, average_dt, global_dt;
+  double t_step;  // simtime at the start of the running step
+  int32_t print_id, it_count, it_print, time_series, time_increment_fixed;
+  int32_t runoff_row, src_idx_low, src_idx_high;
+  int32_t active, halt, events, steps;
+  int32_t cur, src, dst, rd, wr;  // ping-pong state buffers and dt slots
+  int32_t nroff, roff_rows, nsrc, hyg_rows;
+  int32_t status;  // nonzero: a device-side check failed (value = reason)
+  unsigned long long dt_key[2];
+  const double* roff_t;
+  const double* hyg_t;
+};
+
+template <typename T>
+struct StateBufs {
+  T* h[2];
+  T* qx[2];
+  T* qy[2];
+};
+
+// ---------------------------------------------------------------------------
+// k_clock: the per-step scalar work of the reference host loop.
+// ---------------------------------------------------------------------------
+__global__ void k_clock(DevClock* __restrict__ c) {
+  if (threadIdx.x != 0) return;
+  if (c->halt) {
+    c->active = 0;
+    return;
+  }
+  const double t0 = c->simtime;
+  double dt;
+  if (!c->time_increment_fixed) {
+    // compute_global_dt: dry fallback, then clamp to the next print time
+    const unsigned long long key = c->dt_key[c->rd];
+    dt = (key >= kDtKeyInf) ? 1.7976931348623157e308 : __longlong_as_double((long long)key);
+    if (dt >= kMaxValue - 1.0) dt = c->init_dt;
+    const double tp = c->print_interval * (c->print_id + 1);
+    if (t0 + dt > tp) dt = tp - t0;
+  } else {
+    dt = c->time_step;
+  }
+  c->global_dt = dt;
+  c->t_step = t0;
+  c->it_count++;
+  if (c->nroff > 0) {
+    const int last = c->roff_rows - 1;
+    if (t0 > c->roff_t[last]) {
+      c->runoff_row = last;
+    } else if (c->runoff_row + 1 <= last && t0 > c->roff_t[c->runoff_row + 1]) {
+      c->runoff_row++;
+    }
+  }
+  if (c->nsrc > 0) {
+    int lo = c->src_idx_low, hi = c->hyg_rows - 1;
+    bool found = false;
+    for (int i = lo; i < hi; i++) {
+      if (c->hyg_t[i + 1] > t0) {
+        lo = i;
+        hi = i + 1;
+        found = true;
+        break;
+      }
+    }
+    if (!found) lo = hi;
+    c->src_idx_low = lo;
+    c->src_idx_high = hi;
+  }
+  c->src = c->cur;
+  c->dst = c->cur ^ 1;
+  c->cur = c->dst;
+  c->wr = c->rd ^ 1;
+  c->dt_key[c->wr] = kDtKeyInf;
+  c->rd = c->wr;
+  const double t1 = t0 + dt;
+  c->simtime = t1;
+  c->average_dt += dt;
+  c->steps++;
+  int ev = 0;
+  if (c->it_print > 0 && c->it_count % c->it_print == 0) ev |= TRI_EV_LOG;
+  if (c->time_series && t1 - c->last_obs_time >= c->print_observation) ev |= TRI_EV_OBS;
+  if (t1 >= c->print_interval * (c->print_id + 1)) ev |= TRI_EV_PRINT;
+  if (!(t1 < c->sim_duration)) ev |= TRI_EV_END;
+  if (ev) {
+    c->halt = 1;
+    c->events = ev;
+  }
+  c->active = 1;
+}
+
+// ---------------------------------------------------------------------------
+// k_flux_update: one block owns a strip of BW-2 interior columns and RB rows.
+// Thread t holds column c = c0-1+t; threads 0 and BW-1 are the west/east halo
+// columns.  The block marches down its rows keeping the previous row in
+// registers, so every x face and every y face of the strip is evaluated once
+// (plus one halo y row per strip and two halo columns per block):
+//   y face (r, r-1): owner row r, north neighbour row r-1 (kernels_flux.h:359-360)
+//   x face (c-1, c): owner column c-1, east neighbour c   (kernels_flux.h:76-77)
+// A row's update runs once its south face (computed with the next row) is
+// known: h = hn - (xE+yN) - (xW+yS), i.e. hn - rhsh0 - rhsh1 with the
+// reference's rhs0 = flux_x part + flux_y part (kernels_state.h:65).
+// Ghost cells are copied from the source to the destination buffer so both
+// ping-pong buffers keep the boundary state the reference keeps in place.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct RowParts {  // rhs contributions collected for one cell
+  T e0, e1, e2;    // east face, owner part   (flux_x rhs*0)
+  T w0, w1, w2;    // west face, neighbour part (flux_x rhs*1)
+  T n0, n1, n2;    // north face, owner part  (flux_y rhs*0)
+};
+
+template <typename T>
+__device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>& p, T s0, T s1, T s2, T n2v, T dt,
+                                            T hextra, T& ho, T& qxo, T& qyo) {
+  const T E12 = eps12<T>();
+  const T G = T(kGravity);
+  const T hn = c.h;
+  const T rh0 = p.e0 + p.n0, rh1 = p.w0 + s0;
+  T hij = hn - rh0 - rh1;
+  T qxij, qyij;
+  if (hij < T(0)) hij = T(0);
+  if (hij < hextra) {
+    qxij = T(0);
+    qyij = T(0);
+  } else {
+    const T rx0 = p.e1 + p.n1, rx1 = p.w1 + s1;
+    const T ry0 = p.e2 + p.n2, ry1 = p.w2 + s2;
+    const T mx = c.qx - rx0 - rx1;
+    const T my = c.qy - ry0 - ry1;
+    const T modM = dev_sqrt(mx * mx + my * my);
+    if (n2v > E12 && hn >= hextra && modM > E12) {
+      const T tt = dt * G * n2v * modM / (hn * hn * dev_cbrt(hn));
+      const T sq = dev_sqrt(T(1) + T(4) * tt);
+      qxij = T(-0.5) * (mx - mx * sq) / tt;
+      qyij = T(-0.5) * (my - my * sq) / tt;
+    } else {
+      qxij = mx;
+      qyij = my;
+    }
+  }
+  ho = hij;
+  qxo = qxij;
+  qyo = qyij;
+}
+
+template <typename T, int BW>
+__global__ void __launch_bounds__(BW) k_flux_update(const DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                    const T* __restrict__ z, const T* __restrict__ n2,
+                                                    const int32_t* __restrict__ zone, const T* __restrict__ rates,
+                                                    int rows, int cols, int rb, T dx, T hextra) {
+  __shared__ T s_h[BW], s_qx[BW], s_qy[BW], s_z[BW], s_sq[BW], s_u[BW], s_v[BW];
+  __shared__ T s_e0[BW + 1], s_e1[BW + 1], s_e2[BW + 1];
+  if (!clk->active) return;
+  const int src = clk->src, dst = clk->dst;
+  const T dt = T(clk->global_dt);
+  const int nroff = clk->nroff, roff_rows = clk->roff_rows, roff_row = clk->runoff_row;
+  const T* __restrict__ hi = sb.h[src];
+  const T* __restrict__ qxi = sb.qx[src];
+  const T* __restrict__ qyi = sb.qy[src];
+  T* __restrict__ ho = sb.h[dst];
+  T* __restrict__ qxo = sb.qx[dst];
+  T* __restrict__ qyo = sb.qy[dst];
+
+  const int t = threadIdx.x;
+  const int c0 = 1 + blockIdx.x * (BW - 2);
+  const int c = c0 - 1 + t;
+  const int r0 = 1 + blockIdx.y * rb;
+  const int r1 = min(r0 + rb - 1, rows - 2);
+  const bool incol = c < cols;
+  const bool mid = (t >= 1 && t <= BW - 2);
+  const bool upd = mid && c >= 1 && c <= cols - 2;
+  const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this thread
+
+  auto load = [&](int r) -> CellQ<T> {
+    CellQ<T> q;
+    if (incol) {
+      const size_t id = (size_t)r * cols + c;
+      q = make_cell<T>(hi[id], qxi[id], qyi[id], z[id], hextra);
+    } else {
+      q.h = q.qx = q.qy = q.z = q.sq = q.u = q.v = T(0);
+    }
+    return q;
+  };
+  auto copy_ghost = [&](int r) {
+    const size_t id = (size_t)r * cols + c;
+    ho[id] = hi[id];
+    qxo[id] = qxi[id];
+    qyo[id] = qyi[id];
+  };
+
+  CellQ<T> prev = load(r0 - 1);
+  if (r0 - 1 == 0 && incol && (mid || gcol)) copy_ghost(0);
+  RowParts<T> pp;
+  pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
+
+  for (int r = r0; r <= r1 + 1; ++r) {
+    const CellQ<T> cur = load(r);
+    FaceOut<T> Y;
+    Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
+    if (upd) Y = face_flux<T, false>(cur, prev, dx, dt, hextra);
+    if (r - 1 >= r0 && upd) {
+      const size_t id = (size_t)(r - 1) * cols + c;
+      T hn, qn, vn;
+      update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, n2[id], dt, hextra, hn, qn, vn);
+      if (nroff > 0) {  // update_runoff (kernels.h:128-149)
+        const T net = rates[(size_t)zone[id] * roff_rows + roff_row];
+        hn += net * dt;
+        if (hn < hextra) {
+          if (hn < T(0)) hn = T(0);
+          qn = T(0);
+          vn = T(0);
+        }
+      }
+      ho[id] = hn;
+      qxo[id] = qn;
+      qyo[id] = vn;
+    }
+    if (r > r1) {
+      if (r == rows - 1 && incol && (mid || gcol)) copy_ghost(r);
+      break;
+    }
+    // x faces of row r
+    s_h[t] = cur.h;
+    s_qx[t] = cur.qx;
+    s_qy[t] = cur.qy;
+    s_z[t] = cur.z;
+    s_sq[t] = cur.sq;
+    s_u[t] = cur.u;
+    s_v[t] = cur.v;
+    __syncthreads();
+    FaceOut<T> X;
+    X.a0 = X.a1 = X.a2 = X.b0 = X.b1 = X.b2 = T(0);
+    if (t >= 1 && incol && c >= 1) {
+      CellQ<T> left;
+      left.h = s_h[t - 1];
+      left.qx = s_qx[t - 1];
+      left.qy = s_qy[t - 1];
+      left.z = s_z[t - 1];
+      left.sq = s_sq[t - 1];
+      left.u = s_u[t - 1];
+      left.v = s_v[t - 1];
+      X = face_flux<T, true>(left, cur, dx, dt, hextra);
+    }
+    s_e0[t] = X.a0;
+    s_e1[t] = X.a1;
+    s_e2[t] = X.a2;
+    __syncthreads();
+    pp.e0 = s_e0[t + 1 < BW ? t + 1 : t];
+    pp.e1 = s_e1[t + 1 < BW ? t + 1 : t];
+    pp.e2 = s_e2[t + 1 < BW ? t + 1 : t];
+    pp.w0 = X.b0;
+    pp.w1 = X.b1;
+    pp.w2 = X.b2;
+    pp.n0 = Y.a0;
+    pp.n1 = Y.a1;
+    pp.n2 = Y.a2;
+    if (gcol) copy_ghost(r);
+    prev = cur;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse kernels (run on the destination buffer after k_flux_update).
+// 'order' lists the items of one conflict-free wave; items that touch the
+// same cell are in different waves, launched in the reference's index order.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_sources(const DevClock* __restrict__ clk, StateBufs<T> sb, const int32_t* __restrict__ order,
+                          int count, int nsrc, const int32_t* __restrict__ cells, const double* __restrict__ hyg_t,
+                          const T* __restrict__ hyg_v, T dx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count || !clk->active) return;
+  const int id = order[k];
+  const int lo = clk->src_idx_low, hi = clk->src_idx_high;
+  const T dt = T(clk->global_dt);
+  const T simtime = T(clk->t_step);
+  T* h = sb.h[clk->dst];
+  const T flo = hyg_v[(size_t)lo * nsrc + id];
+  const T fhi = hyg_v[(size_t)hi * nsrc + id];
+  const T tlo = T(hyg_t[lo]), thi = T(hyg_t[hi]);
+  T flow;
+  if (lo == hi) {
+    flow = flo;
+  } else {
+    const T td = simtime - tlo;
+    const T td2 = thi - tlo;
+    flow = flo + (((fhi - flo) * td) / td2);
+  }
+  const int sid = cells[id];
+  T hij = h[sid];
+  const T hs = (flow * dt) / (dx * dx);
+  hij += hs;
+  h[sid] = hij;
+}
+
+template <typename T>
+__global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows, int cols) {
+  if (!clk->active) return;
+  const int d = clk->dst;
+  T* h = sb.h[d];
+  T* qx = sb.qx[d];
+  T* qy = sb.qy[d];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // Final values of copy_info_to_exterior_boundaries_west_east followed by
+  // _north_south: ghost columns take the adjacent interior column (rows
+  // 1..rows-2), ghost rows take the adjacent interior row, corners the
+  // diagonal interior cell.
+  auto cp = [&](size_t g, size_t i) {
+    h[g] = h[i];
+    qx[g] = qx[i];
+    qy[g] = qy[i];
+  };
+  if (k < rows) {
+    const int r = k;
+    if (r >= 1 && r <= rows - 2) {
+      cp((size_t)r * cols, (size_t)r * cols + 1);
+      cp((size_t)r * cols + cols - 1, (size_t)r * cols + cols - 2);
+    }
+  }
+  if (k < cols) {
+    const int cc = k;
+    const int ci = cc == 0 ? 1 : (cc == cols - 1 ? cols - 2 : cc);
+    cp((size_t)cc, (size_t)cols + ci);
+    cp((size_t)(rows - 1) * cols + cc, (size_t)(rows - 2) * cols + ci);
+  }
+}
+
+template <typename T>
+__global__ void k_extbc(const DevClock* __restrict__ clk, StateBufs<T> sb, const T* __restrict__ z,
+                        const T* __restrict__ n2, const int32_t* __restrict__ order, int count,
+                        const int32_t* __restrict__ cells, const int32_t* __restrict__ types,
+                        const int32_t* __restrict__ start, const int32_t* __restrict__ nrowsv,
+                        const T* __restrict__ var1, const T* __restrict__ var2, int rows, int cols) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count || !clk->active) return;
+  const int id = order[k];
+  const int d = clk->dst;
+  T* h = sb.h[d];
+  T* qx = sb.qx[d];
+  T* qy = sb.qy[d];
+  const T dt = T(clk->global_dt);
+  const T simtime = T(clk->t_step);
+  const int ii = cells[id];
+  const int bt = types[id];
+  const int s0 = start[id];
+  const int ix = ii / cols, iy = ii % cols;
+  const bool top = (ix == 1), btm = (ix == rows - 2), lt = (iy == 1), rt = (iy == cols - 2);
+  if (!(top || lt || rt || btm)) return;
+  bool corner = false;
+  int ib = ii, ibc = ii;
+  T f0 = T(1), f1 = T(0), f2 = T(0);
+  if (lt) {
+    ib = ii - 1;
+    f1 = T(-1);
+    f2 = T(0);
+  }
+  if (rt) {
+    ib = ii + 1;
+    f1 = T(1);
+    f2 = T(0);
+  }
+  if (top) {
+    ib = ii - cols;
+    f1 = T(0);
+    f2 = T(1);
+    if (lt) {
+      corner = true;
+      ibc = ii - 1;
+      f2 = T(0);
+    }
+    if (rt) {
+      corner = true;
+      ibc = ii + 1;
+      f2 = T(0);
+    }
+  }
+  if (btm) {
+    ib = ii + cols;
+    f1 = T(0);
+    f2 = T(-1);
+    if (lt) {
+      corner = true;
+      ibc = ii - 1;
+      f2 = T(0);
+    }
+    if (rt) {
+      corner = true;
+      ibc = ii + 1;
+      f2 = T(0);
+    }
+  }
+  T hij = h[ii], qxij = qx[ii], qyij = qy[ii];
+  if (bt == 0) {
+    h[ib] = hij;
+    qx[ib] = qxij;
+    qy[ib] = qyij;
+    if (corner) {
+      h[ibc] = hij;
+      qx[ibc] = qxij;
+      qy[ibc] = qyij;
+    }
+    return;
+  }
+  if (bt == 1) {
+    const T lvar = T(0.5) * (simtime + simtime + dt);
+    int lo = 0, hi = nrowsv[id] - 1;
+    if (lvar < var1[s0]) {
+      lo = 0;
+      hi = 0;
+    } else if (lvar > var1[hi + s0]) {
+      lo = hi;
+    } else {
+      lo = 0;  // a non-monotone table leaves the reference's index unset; clamp to row 0
+      for (int i = 0; i < hi; i++) {
+        if (var1[i + s0] <= lvar && var1[i + 1 + s0] > lvar) {
+          lo = i;
+          hi = i + 1;
+          break;
+        }
+      }
+    }
+    T aux;
+    if (lo == hi) {
+      aux = var2[lo + s0];
+    } else {
+      const T td = lvar - var1[lo + s0];
+      const T td2 = var1[hi + s0] - var1[lo + s0];
+      aux = var2[lo + s0] + (((var2[hi + s0] - var2[lo + s0]) * td) / td2);
+    }
+    hij = dev_fmax(aux - z[ii], T(0));
+  } else {
+    const T aux = var1[s0];
+    T vel = T(0);
+    if (bt == 2) vel = dev_sqrt(aux * hij * dev_cbrt(hij) / dev_fmax(n2[ii], T(1e-6)));
+    if (bt == 3) vel = aux * dev_sqrt(T(kGravity) * hij);
+    qxij = hij * vel;
+    qyij = hij * vel;
+  }
+  h[ib] = hij * f0;
+  qx[ib] = qxij * f1;
+  qy[ib] = qyij * f2;
+  h[ii] = hij * f0;
+  qx[ii] = qxij * f1;
+  qy[ii] = qyij * f2;
+  if (corner) {
+    h[ibc] = hij * f0;
+    qx[ibc] = qxij * f1;
+    qy[ibc] = qyij * f2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_wetdry_dt: wet/dry masks and max depth on interior cells, then the CFL dt
+// of every cell (ghosts included, as compute_dt_and_sqrt runs over rows*cols)
+// reduced warp -> block -> one atomicMin on the ordered key of the slot the
+// next k_clock reads.  With WETDRY=false it is the initial dt pass.
+// ---------------------------------------------------------------------------
+template <typename T, bool WETDRY>
+__global__ void __launch_bounds__(256) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                   const T* __restrict__ z, T* __restrict__ maxh, int rows,
+                                                   int cols, T dx, T cn, T hextra) {
+  if (WETDRY && !clk->active) return;
+  const int buf = WETDRY ? clk->dst : clk->cur;
+  const int slot = WETDRY ? clk->wr : clk->rd;
+  const T* __restrict__ h = sb.h[buf];
+  T* __restrict__ qx = sb.qx[buf];
+  T* __restrict__ qy = sb.qy[buf];
+  const T E12 = eps12<T>();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  unsigned long long key = kDtKeyInf;
+  if (r < rows && c < cols) {
+    const size_t id = (size_t)r * cols + c;
+    const T hij = h[id];
+    T qxv = qx[id], qyv = qy[id];
+    if (WETDRY && r >= 1 && r <= rows - 2 && c >= 1 && c <= cols - 2) {
+      const T zij = z[id];
+      if (hij > hextra) {
+        const size_t e = id + 1, w = id - 1, n = id - cols, s = id + cols;
+        if ((hij + zij < z[e] && h[e] < E12) || (hij + zij < z[w] && h[w] < E12)) {
+          qxv = T(0);
+          qx[id] = T(0);
+        }
+        if ((hij + zij < z[n] && h[n] < E12) || (hij + zij < z[s] && h[s] < E12)) {
+          qyv = T(0);
+          qy[id] = T(0);
+        }
+      }
+      if (hij > maxh[id]) maxh[id] = hij;
+    }
+    if (hij > hextra) {
+      const T sq = dev_fmax(dev_sqrt(hij), T(0));
+      const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
+      const T dtc = cn * dx / (maxu + T(kSqrtG) * sq);
+      key = dt_key(dtc);
+    }
+  }
+  // warp -> block -> device minimum
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  __shared__ unsigned long long s_min[32];
+  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+  const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  if (lane == 0) s_min[warp] = key;
+  __syncthreads();
+  if (warp == 0) {
+    key = lane < nwarps ? s_min[lane] : kDtKeyInf;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+      key = other < key ? other : key;
+    }
+    if (lane == 0 && key < kDtKeyInf) atomicMin(&clk->dt_key[slot], key);
+  }
+}
+
+}  // namespace tri
