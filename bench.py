@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Throughput of the TRITON time-stepping hot path on B200: cell-updates/s.
+
+A step is one time step of the reference loop (triton_simulate.h:54-134) over
+the whole grid: CFL dt reduction + dt policy, face fluxes, conserved update,
+wet/dry masks and max depth, all on the GPU.  Workload at N=1: the FP64
+Thacker planar oscillation in a paraboloid bowl, 2048 x 2048 cells, dx 4 m,
+closed walls, CFL 0.5 (seeded-free analytic initial state, synthetic).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation (the
+unmodified TRITON sources compiled with OpenMP into oracle/_ref) on the same
+workload with every host thread.  With N > 1 each rank runs an independent
+replica (the path is not sharded: one domain per GPU), value is the total over
+ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+ALG_BYTES_STEP = {"fp64": 80, "fp32": 40}      # per interior cell and step (whole step)
+ALG_BYTES_FLUX = {"fp64": 64, "fp32": 32}      # flux/update kernel: h,qx,qy,z,n2 read + h,qx,qy written
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "triton_ref_omp")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_per_cell(kernel, precision):
+    """Per-cell DRAM bytes of a kernel from the committed ncu summary
+    (profiles/*.txt line 'traffic_bytes_per_cell <kernel> <precision> <B>')."""
+    pat = re.compile(r"traffic_bytes_per_cell\s+(\S+)\s+(\S+)\s+([0-9.eE+-]+)")
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".txt", ".md")):
+            continue
+        with open(os.path.join(pdir, fn)) as f:
+            for line in f:
+                m = pat.search(line)
+                if m and m.group(1) == kernel and m.group(2) == precision:
+                    return float(m.group(3))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        load = [s for s in sm if s > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def workload(name, n):
+    from triton_b200 import scenarios
+    if name == "thacker":
+        sc = scenarios.thacker(n=n or 2048, dx=4.0)
+        desc = (f"Thacker planar oscillation in a paraboloid bowl, {sc.rows - 2}x{sc.cols - 2} cells, dx 4 m, "
+                f"h0 10 m, a 3000 m, rim amplitude 0.5 m, closed walls, frictionless, CFL 0.5")
+    elif name == "dambreak":
+        sc = scenarios.dambreak(n=n or 512)
+        desc = f"circular dam break {sc.rows - 2}x{sc.cols - 2}, dx 1 m, 10 m inside r=50 m, closed, CFL 0.5"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return sc, desc
+
+
+def cfl_dt0(sc):
+    import numpy as np
+    h, qx, qy = sc.h, sc.qx, sc.qy
+    wet = h > sc.hextra
+    u = np.where(wet, np.maximum(abs(qx), abs(qy)) / np.where(wet, h, 1), 0)
+    dt = np.where(wet, sc.courant * sc.dx / (u + 3.132091953 * np.sqrt(np.where(wet, h, 0))), np.inf)
+    return float(dt.min())
+
+
+def run_reference(sc, steps, threads):
+    """Runs the reference OpenMP build on `sc` for about `steps` time steps;
+    returns (cell-updates/s, iterations, compute seconds)."""
+    from triton_b200 import scenarios
+    if not os.path.exists(REF_EXE):
+        return None
+    tmp = tempfile.mkdtemp(prefix="tri_ref_")
+    try:
+        sc = scenarios.Scenario(**{k: getattr(sc, k) for k in sc.__dataclass_fields__})
+        sc.sim_duration = cfl_dt0(sc) * steps
+        sc.print_interval = sc.sim_duration
+        sc.time_series = 0
+        sc.it_print = 1 << 30
+        cfg = scenarios.write_case(sc, os.path.join(tmp, "input"), fmt="BIN", output_format="BIN")
+        os.makedirs(os.path.join(tmp, "bin"))
+        exe = os.path.join(tmp, "bin", "triton.exe")
+        os.symlink(REF_EXE, exe)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+        p = subprocess.run([exe, cfg], cwd=tmp, env=env, capture_output=True, text=True, timeout=1800)
+        if p.returncode != 0:
+            raise RuntimeError(f"reference run failed: {p.stderr[-2000:]}")
+        its = int(re.findall(r"it:\s*(\d+)", p.stderr)[-1])
+        with open(os.path.join(tmp, "output", "performance.txt")) as f:
+            line = [l for l in f if l.startswith("0,")][0]
+        compute = float(line.split(",")[1])
+        return sc.interior_cells * its / compute, its, compute
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def reference_arm(args, sc, desc):
+    threads = len(os.sched_getaffinity(0))
+    r = run_reference(sc, args.steps + args.warmup, threads)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/triton_ref_omp was not built"}))
+        return
+    val, its, secs = r
+    line = {"metric": METRIC, "value": val, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": its,
+            "warmup": 0, "ms_per_step": 1000.0 * secs / its, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "engine": "reference TRITON sources, OpenMP build, all host threads"},
+            "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                             "sample": f"{its} time steps of the workload ({secs:.2f} s compute)"},
+            "e2e": {"value": val, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="thacker")
+    ap.add_argument("--n", type=int, default=0, help="grid side (default: the workload's full size)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    sc, desc = workload(args.workload, args.n)
+
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args, sc, desc)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from triton_b200 import Domain  # noqa: F401  (fails loudly if the library is missing)
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    stream = torch.cuda.current_stream()
+    d = sc.to_domain(args.precision, stream=stream.cuda_stream)
+    # no events inside the measured steps: the loop never stops to print
+    d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    n, _ = d.advance(args.warmup)
+    assert n == args.warmup
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ
+                           else os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
+    sampler.start()
+    d.set_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    n, ev = d.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    assert n == args.steps, (n, ev)
+    ms = e0.elapsed_time(e1)
+    flux_ms, flux_n, wet_ms, wet_n = d.get_timing()
+    d.set_timing(False)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = sc.interior_cells
+    value = cells * args.steps * world / (ms_max / 1000.0)
+
+    # end to end through the public API from pinned host buffers: upload the
+    # initial fields, run the same number of steps, read the result back
+    import numpy as np
+    host = {k: torch.from_numpy(np.ascontiguousarray(getattr(sc, k), dtype=np.float64)).pin_memory()
+            for k in ("h", "qx", "qy", "z", "n2")}
+    outs = {k: torch.empty(sc.rows * sc.cols, dtype=torch.float64).pin_memory() for k in ("h", "qx", "qy", "maxh")}
+    d2 = sc.to_domain(args.precision, stream=stream.cuda_stream)
+    d2.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    import ctypes as C
+
+    from triton_b200 import _abi
+    L = _abi.lib()
+    fid = {"h": 0, "qx": 1, "qy": 2, "n2": 3, "z": 4, "maxh": 5}
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for k in ("z", "n2", "h", "qx", "qy"):
+        _abi.check(L.tri_domain_upload(d2._h, fid[k], C.cast(host[k].data_ptr(), _abi._dp), sc.rows * sc.cols))
+    _abi.check(L.tri_domain_upload(d2._h, fid["maxh"], C.cast(host["h"].data_ptr(), _abi._dp), sc.rows * sc.cols))
+    n2_, _ = d2.advance(args.steps)
+    for k in ("h", "qx", "qy", "maxh"):
+        _abi.check(L.tri_domain_download(d2._h, fid[k], C.cast(outs[k].data_ptr(), _abi._dp), sc.rows * sc.cols))
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ems = f0.elapsed_time(f1)
+    te = torch.tensor([ems], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = cells * n2_ * world / (float(te.item()) / 1000.0)
+    h2d = 6 * sc.rows * sc.cols * 8
+    d2h = 4 * sc.rows * sc.cols * 8
+    d2.close()
+
+    peak, peak_kind = _peaks()
+    flux_avg_s = (flux_ms / max(flux_n, 1)) / 1000.0
+    achieved = ALG_BYTES_FLUX[args.precision] * cells / flux_avg_s / 1e9
+    tpc = _traffic_per_cell("flux_update", args.precision)
+    step_gbs = ALG_BYTES_STEP[args.precision] * cells * args.steps / (ms / 1000.0) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = len(os.sched_getaffinity(0))
+        r = run_reference(sc, 60, threads)
+        if r is not None:
+            cpu = {"value": r[0], "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                   "sample": f"{r[1]} time steps of the same workload, reference OpenMP build ({r[2]:.2f} s compute)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "data": "synthetic",
+            "config": {"workload": desc, "grid": [sc.rows - 2, sc.cols - 2], "interior_cells": cells,
+                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state ~%d MB per GPU)" % (sc.rows * sc.cols * 72 // 2 ** 20)},
+            "roofline": {"bound": "hbm", "kernel": "k_flux_update", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (tpc * cells) if tpc is not None else None,
+                         "algorithmic_bytes_per_launch": ALG_BYTES_FLUX[args.precision] * cells,
+                         "avg_launch_ms": flux_avg_s * 1000.0, "peak_source": f"MEASURED_PEAKS.json hbm_gbs "
+                                                                               f"({peak_kind})",
+                         "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
+                         "wetdry_dt_avg_launch_ms": wet_ms / max(wet_n, 1)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d / max(n2_, 1),
+                    "d2h_bytes_per_step": d2h / max(n2_, 1)},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    d.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -76,9 +76,13 @@ def run_lockstep(sc, precision="fp64", exact=True, max_events=10 ** 6, chunk=10 
             n2, e2 = d.advance(chunk)
             assert (n1, e1) == (n2, e2), f"oracle ran {n1} steps (events {e1}), gpu {n2} (events {e2})"
             c = d.get_clock()
-            assert c.simtime == o.s.simtime, f"simtime gpu {c.simtime!r} oracle {o.s.simtime!r}"
             assert c.it_count == o.s.it_count
-            assert c.average_dt == o.s.average_dt
+            if exact:
+                assert c.simtime == o.s.simtime, f"simtime gpu {c.simtime!r} oracle {o.s.simtime!r}"
+                assert c.average_dt == o.s.average_dt
+            else:  # dt follows the state, which may differ in the last bits (cbrt)
+                assert abs(c.simtime - o.s.simtime) <= REL_TOL * max(abs(o.s.simtime), 1.0)
+                assert abs(c.average_dt - o.s.average_dt) <= REL_TOL * max(abs(o.s.average_dt), 1e-3)
             steps += n1
             nev += 1
             if check_every_event or e1 & EV_END:

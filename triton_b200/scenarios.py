@@ -253,12 +253,122 @@ def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, r
                     meta=dict(n=n, seed=seed))
 
 
+def extbc_segments(sc, segments):
+    """Builds the external-boundary tables the reference derives from an
+    .extbc file (process_boundary_condition, triton_init.h:869-1055) and
+    applies its ghost-cell preprocessing (matrix.h:869-926 for the DEM and
+    triton_init.h:1250-1289 for DEM/h/qx/qy).
+
+    segments: list of (type, (row1, col1), (row2, col2), value) in interior
+    0-based cell coordinates along one edge; value is the Froude number
+    (type 3), the slope (type 2), ignored for type 0, or for type 1 a list of
+    (hours, water level) rows.  Cells are listed from the lower to the higher
+    row/column index, segment by segment, as create_involved_cells does."""
+    R, C = sc.rows - 2, sc.cols - 2
+    Cp = sc.cols
+    cells, types, start, nrows, var1, var2 = [], [], [], [], [], []
+    for bt, (r1, c1), (r2, c2), val in segments:
+        if c1 == c2:
+            loc = 0 if c1 == 0 else 2
+            pts = [(r, c1) for r in range(min(r1, r2), max(r1, r2) + 1)]
+        elif r1 == r2:
+            loc = 1 if r1 == 0 else 3
+            pts = [(r1, c) for c in range(min(c1, c2), max(c1, c2) + 1)]
+        else:
+            raise ValueError("segment must follow one edge")
+        if bt == 1:
+            rows_h = [(float(t), float(v)) for t, v in val]
+            t_s = [t * 3600.0 for t, _ in rows_h]  # extBC::convert_to_secs
+            lv = [v for _, v in rows_h]
+        else:
+            t_s = [float(val or 0.0)]
+            lv = [float(val or 0.0)]
+        s0 = len(var1)
+        var1 += t_s
+        var2 += lv
+        for r, c in pts:
+            cells.append((r + 1) * Cp + c + 1)
+            types.append(bt)
+            start.append(s0)
+            nrows.append(len(t_s))
+        # DEM ghosts next to the segment (copy_value_into_ghost_cells_location)
+        z = sc.z
+        for r, c in pts:
+            ix, iy = r + 1, c + 1
+            if loc == 0:
+                z[ix, iy - 1] = z[ix, iy]
+            if loc == 2:
+                z[ix, iy + 1] = z[ix, iy]
+            if loc == 1:
+                z[ix - 1, iy] = z[ix, iy]
+            if loc == 3:
+                z[ix + 1, iy] = z[ix, iy]
+            v = z[ix, iy]
+            if r == 0 and c == 0:
+                z[0, 0] = z[0, 1] = z[1, 0] = v
+            if r == 0 and c == C - 1:
+                z[0, Cp - 2] = z[0, Cp - 1] = z[1, Cp - 1] = v
+            if r == R - 1 and c == 0:
+                z[sc.rows - 2, 0] = z[sc.rows - 1, 0] = z[sc.rows - 1, 1] = v
+            if r == R - 1 and c == C - 1:
+                z[sc.rows - 2, Cp - 1] = z[sc.rows - 1, Cp - 2] = z[sc.rows - 1, Cp - 1] = v
+        if not hasattr(sc, "_segments"):
+            sc._segments = []
+        sc._segments.append((bt, (r1, c1), (r2, c2), val))
+    # per-cell ghost copies of DEM, h, qx, qy (triton_init.h:1250-1289)
+    for ii in cells:
+        ix, iy = divmod(ii, Cp)
+        nb = []
+        if iy == 1:
+            nb.append(ii - 1)
+        if iy == Cp - 2:
+            nb.append(ii + 1)
+        if ix == 1:
+            nb.append(ii - Cp)
+        if ix == sc.rows - 2:
+            nb.append(ii + Cp)
+        for g in nb:
+            for a in (sc.z, sc.h, sc.qx, sc.qy):
+                a.flat[g] = a.flat[ii]
+    sc.extbc = dict(cells=np.array(cells, np.int32), types=np.array(types, np.int32),
+                    start=np.array(start, np.int32), nrows=np.array(nrows, np.int32),
+                    var1=np.array(var1, dtype=np.float64), var2=np.array(var2, dtype=np.float64))
+    return sc
+
+
+def sources_table(sc, cells_rc, times_h, flows):
+    """Point sources at interior cells (row, col) with a hydrograph given in
+    hours and m3/s (hydrograph::convert_time_hr_to_secs, inflow.h:260-272)."""
+    Cp = sc.cols
+    times_h = np.asarray(times_h, dtype=np.float64)
+    flows = np.asarray(flows, dtype=np.float64).reshape(times_h.size, len(cells_rc))
+    sc.sources = dict(cells=np.array([(r + 1) * Cp + c + 1 for r, c in cells_rc], np.int32),
+                      times=times_h * 3600.0, flows=flows.reshape(-1), times_h=times_h, flows_rows=flows,
+                      cells_rc=list(cells_rc))
+    return sc
+
+
+def runoff_table(sc, zone_interior, times_h, rates_mm_h):
+    """Runoff zones with rates in mm/h per zone (columns) and time rows in
+    hours, converted as read_inflows does (triton_init.h:155-162:
+    hours->s, then /3600, then *0.001)."""
+    times_h = np.asarray(times_h, dtype=np.float64)
+    mm = np.asarray(rates_mm_h, dtype=np.float64).reshape(times_h.size, -1)
+    nz = mm.shape[1]
+    zone = np.zeros((sc.rows, sc.cols), dtype=np.int32)
+    zone[1:-1, 1:-1] = zone_interior
+    si = (mm / 3600.0) * 0.001
+    sc.runoff = dict(zone=zone, times=times_h * 3600.0, rates=np.ascontiguousarray(si.T).reshape(-1), nzones=nz,
+                     times_h=times_h, rates_mm_h=mm)
+    return sc
+
+
 def mixed(rows=37, cols=53, dx=5.0, seed=7, open_boundaries=0, friction=True, with_sources=True,
           with_runoff=True, with_extbc=True, duration=30.0, wet_fraction=0.5):
     """Small random case that drives every forcing path of the step: rough
     terrain with partly wet cells, friction, two sources sharing a cell,
-    zoned runoff, external boundary cells of types 0-3 (two segments sharing
-    a corner) and optional open boundaries."""
+    zoned runoff, external boundary cells of types 0-3 (segments sharing
+    corners) and optional open boundaries."""
     rng = np.random.default_rng(seed)
     R, C = rows, cols
     dem = _value_noise(rng, R, C, octaves=4) * 2.0 + 5.0
@@ -275,52 +385,172 @@ def mixed(rows=37, cols=53, dx=5.0, seed=7, open_boundaries=0, friction=True, wi
     sc = Scenario("mixed", dx, z, hp, qxp, qyp, n2, courant=0.5, hextra=0.001, open_boundaries=open_boundaries,
                   sim_duration=duration, print_interval=duration / 3, print_observation=duration / 7,
                   time_series=1, it_print=25)
-    Cp = C + 2
+    sc.meta["mann"] = mann
     if with_runoff:
         nz = 3
-        zone = np.zeros((R + 2, C + 2), dtype=np.int32)
-        zone[1:-1, 1:-1] = rng.integers(0, nz, (R, C))
-        t = np.array([0.0, 4.0, 9.0, 15.0, 1e5])
-        rates = (rng.random((nz, t.size)) * 40.0 - 5.0) / 3600.0 * 0.001  # includes small negative rates
-        sc.runoff = dict(zone=zone, times=t, rates=rates.reshape(-1), nzones=nz)
+        t_h = np.array([0.0, 0.001, 0.0025, 0.004, 30.0])
+        mm = np.round(rng.random((t_h.size, nz)) * 40.0 - 5.0, 3)  # includes small negative rates
+        runoff_table(sc, rng.integers(0, nz, (R, C)), t_h, mm)
     if with_sources:
-        cells = np.array([(R // 3 + 1) * Cp + C // 4 + 1, (2 * R // 3 + 1) * Cp + C // 2 + 1,
-                          (R // 3 + 1) * Cp + C // 4 + 1], dtype=np.int32)
-        t = np.array([0.0, 5.0, 12.0, 20.0, 1e5])
-        flows = rng.random((t.size, cells.size)) * 2.0
-        sc.sources = dict(cells=cells, times=t, flows=flows.reshape(-1))
+        cells_rc = [(R // 3, C // 4), (2 * R // 3, C // 2), (R // 3, C // 4)]
+        t_h = np.array([0.0, 0.0015, 0.003, 0.006, 30.0])
+        flows = np.round(rng.random((t_h.size, len(cells_rc))) * 2.0, 4)
+        sources_table(sc, cells_rc, t_h, flows)
     if with_extbc:
-        # east column: type 1 level series; north row: type 3 (Froude) from the
-        # NE corner it shares with the east segment, then type 2 (normal
-        # slope); west column: type 2; south row: type 0 (open copy)
-        cells, types, start, nrows = [], [], [], []
-        var1, var2 = [], []
-        t1 = [0.0, 6.0, 14.0, 1e5]
-        l1 = [6.0, 7.0, 6.5, 6.5]
-        s1 = len(var1)
-        var1 += t1
-        var2 += l1
-        for r in range(1, R + 1):
-            cells.append(r * Cp + C); types.append(1); start.append(s1); nrows.append(len(t1))
-        s3 = len(var1)
-        var1 += [0.8]
-        var2 += [0.8]
-        for c in range(C, C // 2, -1):
-            cells.append(1 * Cp + c); types.append(3); start.append(s3); nrows.append(1)
-        s2 = len(var1)
-        var1 += [0.002]
-        var2 += [0.002]
-        for c in range(C // 2, 0, -1):
-            cells.append(1 * Cp + c); types.append(2); start.append(s2); nrows.append(1)
-        for r in range(2, R + 1):
-            cells.append(r * Cp + 1); types.append(2); start.append(s2); nrows.append(1)
-        s0 = len(var1)
-        var1 += [0.0]
-        var2 += [0.0]
-        for c in range(2, C):
-            cells.append(R * Cp + c); types.append(0); start.append(s0); nrows.append(1)
-        sc.extbc = dict(cells=np.array(cells, np.int32), types=np.array(types, np.int32),
-                        start=np.array(start, np.int32), nrows=np.array(nrows, np.int32),
-                        var1=np.array(var1), var2=np.array(var2))
+        # east column: type 1 water level series; north row: type 3 (Froude)
+        # sharing the NE corner, then type 2 (normal slope); west column:
+        # type 2; south row: type 0 (open copy)
+        extbc_segments(sc, [
+            (1, (0, C - 1), (R - 1, C - 1), [(0.0, 6.0), (0.0017, 7.0), (0.0039, 6.5), (30.0, 6.5)]),
+            (3, (0, C // 2), (0, C - 1), 0.8),
+            (2, (0, 0), (0, C // 2 - 1), 0.002),
+            (2, (1, 0), (R - 1, 0), 0.002),
+            (0, (R - 1, 1), (R - 1, C - 2), None),
+        ])
+    Cp = C + 2
     sc.obs_cells = np.array([(R // 2 + 1) * Cp + C // 2 + 1, (2 + 1) * Cp + 3, (R) * Cp + C], dtype=np.int32)
+    sc.meta["obs_rc"] = [(R // 2, C // 2), (2, 2), (R - 1, C - 1)]
     return sc
+
+
+# ---------------------------------------------------------------------------
+def _write_raster(path, a, fmt, dem_header=None, dtype=np.float64):
+    """Interior raster in the reference's formats: ASCII rows separated by
+    single spaces (matrix_io.h:77-149; the DEM adds a 6-line header,
+    dem_utils.h:163-228) or binary (a header of 2 values, rows and cols, or
+    6 DEM header values, in the raster's type, then row-major data,
+    matrix_io.h:225-286)."""
+    if fmt == "BIN":
+        if dem_header is not None:
+            hdr = np.array(dem_header, dtype=dtype)
+        else:
+            hdr = np.array([a.shape[0], a.shape[1]], dtype=dtype)
+        with open(path, "wb") as f:
+            hdr.tofile(f)
+            np.ascontiguousarray(a, dtype=dtype).tofile(f)
+    else:
+        with open(path, "w") as f:
+            if dem_header is not None:
+                names = ["ncols", "nrows", "xllcorner", "yllcorner", "cellsize", "NODATA_value"]
+                for k, v in zip(names, dem_header):
+                    f.write(f"{k} {v!r}\n" if isinstance(v, float) else f"{k} {v}\n")
+            for row in a:
+                if dtype == np.int32:
+                    f.write(" ".join(str(int(v)) for v in row) + "\n")
+                else:  # repr keeps the double exactly; a '.' marks it as floating point
+                    f.write(" ".join(_fmt(v) for v in row) + "\n")
+
+
+def _fmt(v):
+    s = repr(float(v))
+    if "." not in s:
+        if "e" in s or "E" in s:
+            m, e = s.lower().split("e")
+            s = f"{m}.0e{e}"
+        else:
+            s += ".0"
+    return s
+
+
+def write_case(sc, directory, fmt="BIN", output_format="BIN", output_folder="output", name=None,
+               max_value_print=""):
+    """Writes `sc` as a reference-format case (cfg + inputs) into `directory`
+    and returns the cfg path.  Paths inside the cfg are absolute.  The
+    reference recovers the same padded arrays and tables from these files
+    (initial fields, walls, Manning squared, forcing unit conversions, cell
+    coordinates -> indices via calc_src_col/row)."""
+    os.makedirs(directory, exist_ok=True)
+    name = name or sc.name
+    R, C = sc.rows - 2, sc.cols - 2
+    dx = sc.dx
+    P = lambda f: os.path.abspath(os.path.join(directory, f))
+    ext = "bin" if fmt == "BIN" else "asc"
+    _write_raster(P(f"{name}.dem.{ext}"), sc.z[1:-1, 1:-1], fmt,
+                  dem_header=[float(C), float(R), sc.xll, sc.yll, dx, -9999.0] if fmt == "BIN" else
+                  [C, R, sc.xll, sc.yll, dx, -9999])
+    _write_raster(P(f"{name}.h.{ext}"), sc.h[1:-1, 1:-1], fmt)
+    _write_raster(P(f"{name}.qx.{ext}"), sc.qx[1:-1, 1:-1], fmt)
+    _write_raster(P(f"{name}.qy.{ext}"), sc.qy[1:-1, 1:-1], fmt)
+    mann = sc.meta.get("mann")
+    if mann is None:
+        mann = np.sqrt(sc.n2[1:-1, 1:-1])
+    _write_raster(P(f"{name}.mann.{ext}"), mann, fmt)
+
+    def xy(r, c):
+        return sc.xll + (c + 0.5) * dx, sc.yll + (R - r - 0.5) * dx
+
+    cfg = {
+        "dem_filename": P(f"{name}.dem.{ext}"), "input_format": fmt, "input_option": "SEQ",
+        "outfile_pattern": "%s/%s/%s_%02d_%02d", "output_format": output_format, "output_option": "SEQ",
+        "output_folder": output_folder, "n_infile": P(f"{name}.mann.{ext}"), "const_mann": "0.0",
+        "h_infile": P(f"{name}.h.{ext}"), "qx_infile": P(f"{name}.qx.{ext}"), "qy_infile": P(f"{name}.qy.{ext}"),
+        "num_sources": "0", "num_runoffs": "0", "num_extbc": "0", "time_series_flag": str(int(sc.time_series)),
+        "print_option": "huv", "sim_start_time": "0", "sim_duration": repr(float(sc.sim_duration)),
+        "checkpoint_id": "0", "time_increment_fixed": "0", "time_step": repr(float(sc.time_step)),
+        "print_interval": repr(float(sc.print_interval)), "it_print": str(int(sc.it_print)), "it_count": "0",
+        "courant": repr(float(sc.courant)), "hextra": repr(float(sc.hextra)), "gpu_direct_flag": "0",
+        "domain_decomposition": "static", "factor_interval_domain_decomposition": "2",
+        "open_boundaries": str(int(sc.open_boundaries)),
+    }
+    if max_value_print:  # the reference's cfg parser needs a value after '=' (config_utils.h:216-219)
+        cfg["max_value_print_option"] = max_value_print
+    if sc.time_series:
+        cfg["print_observation"] = repr(float(sc.print_observation))
+        rc = sc.meta.get("obs_rc")
+        if rc is None:
+            rc = [divmod(int(i), sc.cols) for i in sc.obs_cells]
+            rc = [(r - 1, c - 1) for r, c in rc]
+        with open(P(f"{name}.obs"), "w") as f:
+            f.write("%X-Location,Y-Location\n")
+            for r, c in rc:
+                x, y = xy(r, c)
+                f.write(f"{x!r},{y!r}\n")
+        cfg["observation_loc_file"] = P(f"{name}.obs")
+    if sc.sources is not None and len(sc.sources["cells"]):
+        s = sc.sources
+        rcs = s.get("cells_rc") or [((int(i) // sc.cols) - 1, (int(i) % sc.cols) - 1) for i in s["cells"]]
+        with open(P(f"{name}.src"), "w") as f:
+            f.write("%X-Location,Y-Location\n")
+            for r, c in rcs:
+                x, y = xy(r, c)
+                f.write(f"{x!r},{y!r}\n")
+        with open(P(f"{name}.hyg"), "w") as f:
+            f.write("% Time(hr), Discharge(cms)\n")
+            for t, row in zip(s["times_h"], s["flows_rows"]):
+                f.write(",".join([repr(float(t))] + [repr(float(v)) for v in row]) + "\n")
+        cfg.update(num_sources=str(len(rcs)), src_loc_file=P(f"{name}.src"), hydrograph_filename=P(f"{name}.hyg"))
+    if sc.runoff is not None:
+        r = sc.runoff
+        _write_raster(P(f"{name}.rmap.{ext}"), r["zone"][1:-1, 1:-1], fmt, dtype=np.int32)
+        with open(P(f"{name}.roff"), "w") as f:
+            f.write("% Time(hr), Rate(mm/hr)\n")
+            for t, row in zip(r["times_h"], r["rates_mm_h"]):
+                f.write(",".join([repr(float(t))] + [repr(float(v)) for v in np.atleast_1d(row)]) + "\n")
+        cfg.update(num_runoffs=str(int(r["nzones"])), runoff_filename=P(f"{name}.roff"),
+                   runoff_map=P(f"{name}.rmap.{ext}"))
+    segs = getattr(sc, "_segments", None)
+    if segs:
+        lines = ["% BC Type, X1, Y1, X2, Y2, BC"]
+        for k, (bt, (r1, c1), (r2, c2), val) in enumerate(segs):
+            x1, y1 = xy(r1, c1)
+            x2, y2 = xy(r2, c2)
+            if bt == 1:
+                fn = f"{name}_bc{k}.txt"
+                with open(P(fn), "w") as f:
+                    f.write("% Time(hr), WSE(m)\n")
+                    for t, v in val:
+                        f.write(f"{float(t)!r},{float(v)!r}\n")
+                tail = fn
+            elif bt == 0:
+                tail = "0"
+            else:
+                tail = repr(float(val))
+            lines.append(f"{bt},{x1!r},{y1!r},{x2!r},{y2!r},{tail}")
+        with open(P(f"{name}.extbc"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+        cfg.update(num_extbc=str(len(segs)), extbc_file=P(f"{name}.extbc"), extbc_dir=os.path.abspath(directory))
+    path = P(f"{name}.cfg")
+    with open(path, "w") as f:
+        for k, v in cfg.items():
+            f.write(f"{k}={v}\n")
+    return path
