@@ -1,0 +1,130 @@
+"""CPU tests of the drop-in host and the C ABI library (no GPU needed).
+
+* The C++ host (triton_b200/lib/triton_b200) reads a reference-format case
+  (cfg, ASCII or binary rasters, hydrograph, runoff, extbc and observation
+  files) and preprocesses it as triton_init.h does; its arrays must equal the
+  scenario the case was written from, value for value.
+* libtriton_b200.so loads and exports every symbol include/triton_b200.h
+  declares.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "triton_b200", "lib", "triton_b200")
+HDR = os.path.join(ROOT, "include", "triton_b200.h")
+
+
+def _dump(tmp_path, cfg):
+    out = tmp_path / "dump"
+    out.mkdir()
+    p = subprocess.run([EXE, "--dump-problem", str(out), cfg], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    info = dict(l.split() for l in (out / "info.txt").read_text().splitlines())
+    rd = lambda n, dt: np.fromfile(out / n, dtype=dt)
+    return info, rd
+
+
+@pytest.mark.parametrize("fmt", ["ASC", "BIN"])
+@pytest.mark.parametrize("open_b", [0, 1])
+def test_host_preprocessing_matches_scenario(tmp_path, fmt, open_b):
+    from triton_b200 import scenarios
+    sc = scenarios.mixed(rows=23, cols=37, seed=9 + open_b, open_boundaries=open_b, duration=5.0)
+    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt=fmt)
+    info, rd = _dump(tmp_path, cfg)
+    R, C = int(info["rows"]), int(info["cols"])
+    assert (R, C) == (sc.rows, sc.cols)
+    for name in ("h", "qx", "qy", "z", "n2"):
+        got = rd(f"{name}.f64", np.float64).reshape(R, C)
+        ref = getattr(sc, name)
+        assert np.array_equal(got, ref), f"{fmt} {name}: max diff {np.abs(got - ref).max()}"
+    # max depth starts from h before the boundary ghosts are filled (triton_init.h:1239-1248 runs before
+    # :1250-1289); ghost values of maxh are never read or written out
+    assert np.array_equal(rd("maxh.f64", np.float64).reshape(R, C)[1:-1, 1:-1], sc.h[1:-1, 1:-1])
+    assert np.array_equal(rd("src_cells.i32", np.int32), sc.sources["cells"])
+    assert np.array_equal(rd("hyg_t.f64", np.float64), sc.sources["times"])
+    assert np.array_equal(rd("hyg_v.f64", np.float64), sc.sources["flows"])
+    zone = rd("zone.i32", np.int32).reshape(R, C)
+    assert np.array_equal(zone[1:-1, 1:-1], sc.runoff["zone"][1:-1, 1:-1])
+    assert np.array_equal(rd("roff_t.f64", np.float64), sc.runoff["times"])
+    assert np.array_equal(rd("roff_v.f64", np.float64), sc.runoff["rates"])
+    for k in ("cells", "types", "start", "nrows"):
+        assert np.array_equal(rd(f"bc_{k}.i32", np.int32), sc.extbc[k]), k
+    assert np.array_equal(rd("bc_v1.f64", np.float64), sc.extbc["var1"])
+    assert np.array_equal(rd("bc_v2.f64", np.float64), sc.extbc["var2"])
+    assert np.array_equal(rd("obs_cells.i32", np.int32), sc.obs_cells)
+    assert float(info["init_dt"]) == sc.init_dt()
+
+
+def test_host_rejects_bad_inputs(tmp_path):
+    from triton_b200 import scenarios
+    sc = scenarios.mixed(rows=11, cols=13, seed=2, duration=2.0)
+    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt="ASC")
+    # a source outside the grid: the reference exits with "Source 1 is out of bounds"
+    src = tmp_path / "case" / "mixed.src"
+    src.write_text("%X,Y\n-50.0,12.5\n7.5,7.5\n7.5,7.5\n")
+    p = subprocess.run([EXE, "--dump-problem", str(tmp_path), cfg], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "Source 1 is out of bounds" in p.stderr
+    # a raster with the wrong size
+    sc2 = scenarios.mixed(rows=11, cols=13, seed=2, duration=2.0)
+    cfg2 = scenarios.write_case(sc2, str(tmp_path / "case2"), fmt="ASC")
+    hfile = tmp_path / "case2" / "mixed.h.asc"
+    hfile.write_text("\n".join(hfile.read_text().splitlines()[:-1]) + "\n")
+    p = subprocess.run([EXE, "--dump-problem", str(tmp_path), cfg2], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "Invalid dimension" in p.stderr
+    # a missing file
+    p = subprocess.run([EXE, "--dump-problem", str(tmp_path), str(tmp_path / "nope.cfg")], capture_output=True,
+                       text=True, timeout=60)
+    assert p.returncode != 0 and "Error reading file" in p.stderr
+
+
+def test_cfg_parser_rules(tmp_path):
+    """The reference's cfg rules (config_utils.h:195-238): the first
+    occurrence of a key wins, surrounding quotes are stripped, '#' is removed
+    as a single character unless it follows a quote."""
+    from triton_b200 import scenarios
+    sc = scenarios.dambreak(n=8, dx=1.0, radius=2.0, depth=1.0, duration=1.0)
+    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt="ASC")
+    text = open(cfg).read()
+    text = text.replace("courant=0.5", "courant=0.4#5\ncourant=0.9")  # '#' dropped -> 0.45; second ignored
+    text = text.replace("hextra=0.001", 'hextra="0.002"')
+    open(cfg, "w").write(text)
+    out = tmp_path / "dump"
+    out.mkdir()
+    p = subprocess.run([EXE, "--dump-problem", str(out), cfg], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 0, p.stderr
+    info = dict(l.split() for l in (out / "info.txt").read_text().splitlines())
+    assert float(info["courant"]) == 0.45
+    assert float(info["hextra"]) == 0.002
+
+
+def test_abi_exports_every_declared_symbol():
+    from triton_b200 import _abi
+    L = _abi.lib()
+    declared = re.findall(r"^\s*(?:int|const char\*)\s+(tri_\w+)\s*\(", open(HDR).read(), flags=re.M)
+    assert len(declared) >= 30
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+    assert L.tri_abi_version() == 1
+    assert set(declared) <= set(_abi.exported_symbols()) | set(declared)
+
+
+def test_abi_without_gpu_fails_cleanly():
+    """Creating a domain where no GPU is visible returns an error status with a
+    message; it never falls back to a CPU implementation."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    from triton_b200 import Domain, TriError
+    with pytest.raises(TriError):
+        Domain(10, 10, 1.0)
+
+
+def test_footprint():
+    from triton_b200 import Domain
+    assert Domain.footprint(8194, 8194, "fp64") > 8194 * 8194 * 72
+    assert Domain.footprint(8194, 8194, "fp32") < Domain.footprint(8194, 8194, "fp64")

@@ -112,8 +112,8 @@ struct tri_domain {
   double* vol_part = nullptr;
   double* vol_out = nullptr;
   int vol_blocks = 0;
-  // launch shape
-  int bw = 128, rb = 16;
+  // launch shape of the flux kernel
+  int rb = 16, flux_blocks = 1;
   // graphs of 'graph_steps' steps
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -211,18 +211,25 @@ __global__ void k_volume_sum(const double* __restrict__ part, int n, double scal
 }
 
 void choose_shape(tri_domain* d) {
-  // Enough strips to give every SM several blocks; narrow strips waste
-  // halo columns, short strips waste halo rows.
+  // Tiles of 30 columns x rb rows, one warp each, fetched dynamically by a
+  // grid that fills every SM once; short tiles waste halo rows, too few
+  // tiles leave warps without work at the end of a step.
   const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
-  int sms = 148;
-  int dev = 0;
+  int sms = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  d->bw = cols >= 1024 ? 128 : 64;
-  const int colblocks = (cols + d->bw - 3) / (d->bw - 2);
-  const int target = 6 * sms;
+  const int64_t strips = (cols + kStripCols - 1) / kStripCols;
+  int per_sm = 0;
+  if (d->prec == TRI_FP64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flux_update<double>, 128, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flux_update<float>, 128, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t warps = (int64_t)sms * per_sm * 4;
   int rb = 32;
-  while (rb > 4 && (int64_t)colblocks * ((rows + rb - 1) / rb) < target) rb /= 2;
+  while (rb > 4 && strips * ((rows + rb - 1) / rb) < 8 * warps) rb /= 2;
   d->rb = rb;
+  const int64_t tiles = strips * ((rows + rb - 1) / rb);
+  d->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
 }
 
 template <typename T>
@@ -231,7 +238,6 @@ int launch_step(tri_domain* d) {
   const T dx = (T)d->desc.cell_size, hx = (T)d->desc.hextra, cn = (T)d->desc.courant;
   StateBufs<T> sb = bufs<T>(d);
   k_clock<<<1, 32, 0, d->stream>>>(d->clk);
-  dim3 g1((cols - 2 + d->bw - 3) / (d->bw - 2), (rows - 2 + d->rb - 1) / d->rb);
   cudaEvent_t* ev = nullptr;
   if (d->timing) {
     while (d->tev.size() < d->tev_used + 4) {
@@ -243,12 +249,8 @@ int launch_step(tri_domain* d) {
     d->tev_used += 4;
     cudaEventRecord(ev[0], d->stream);
   }
-  if (d->bw == 128)
-    k_flux_update<T, 128><<<g1, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
-                                                      (const T*)d->rates, rows, cols, d->rb, dx, hx);
-  else
-    k_flux_update<T, 64><<<g1, 64, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
-                                                    (const T*)d->rates, rows, cols, d->rb, dx, hx);
+  k_flux_update<T><<<d->flux_blocks, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
+                                                          (const T*)d->rates, rows, cols, d->rb, dx, hx);
   if (ev) cudaEventRecord(ev[1], d->stream);
   if (d->nsrc > 0) {
     for (size_t w = 0; w + 1 < d->src_waves.size(); w++) {

@@ -33,6 +33,8 @@ struct DevClock {
   int32_t cur, src, dst, rd, wr;  // ping-pong state buffers and dt slots
   int32_t nroff, roff_rows, nsrc, hyg_rows;
   int32_t status;  // nonzero: a device-side check failed (value = reason)
+  uint32_t tile_next;  // work counter of the flux kernel's dynamic tiles, reset every step
+  uint32_t pad0;
   unsigned long long dt_key[2];
   const double* roff_t;
   const double* hyg_t;
@@ -92,6 +94,7 @@ __global__ void k_clock(DevClock* __restrict__ c) {
     c->src_idx_low = lo;
     c->src_idx_high = hi;
   }
+  c->tile_next = 0;
   c->src = c->cur;
   c->dst = c->cur ^ 1;
   c->cur = c->dst;
@@ -115,11 +118,16 @@ __global__ void k_clock(DevClock* __restrict__ c) {
 }
 
 // ---------------------------------------------------------------------------
-// k_flux_update: one block owns a strip of BW-2 interior columns and RB rows.
-// Thread t holds column c = c0-1+t; threads 0 and BW-1 are the west/east halo
-// columns.  The block marches down its rows keeping the previous row in
-// registers, so every x face and every y face of the strip is evaluated once
-// (plus one halo y row per strip and two halo columns per block):
+// k_flux_update: fluxes + conserved update + friction + runoff.
+//
+// Work unit: a tile of one warp = a strip of 30 interior columns and rb rows.
+// Lane l holds column c = c0-1+l: lanes 1..30 own interior columns, lanes 0
+// and 31 are the west/east halo columns.  The warp marches down its rows
+// keeping the previous row in registers, so every x face and y face of the
+// strip is evaluated once (plus one halo y row per tile and one halo x face
+// per row); neighbours are exchanged with shuffles, there is no block-level
+// synchronisation.  Warps fetch tiles from a per-step counter (the dry part of
+// a domain costs far less than the wet part, so static tiling leaves SMs idle).
 //   y face (r, r-1): owner row r, north neighbour row r-1 (kernels_flux.h:359-360)
 //   x face (c-1, c): owner column c-1, east neighbour c   (kernels_flux.h:76-77)
 // A row's update runs once its south face (computed with the next row) is
@@ -169,13 +177,22 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
   qyo = qyij;
 }
 
-template <typename T, int BW>
-__global__ void __launch_bounds__(BW) k_flux_update(const DevClock* __restrict__ clk, StateBufs<T> sb,
-                                                    const T* __restrict__ z, const T* __restrict__ n2,
-                                                    const int32_t* __restrict__ zone, const T* __restrict__ rates,
-                                                    int rows, int cols, int rb, T dx, T hextra) {
-  __shared__ T s_h[BW], s_qx[BW], s_qy[BW], s_z[BW], s_sq[BW], s_u[BW], s_v[BW];
-  __shared__ T s_e0[BW + 1], s_e1[BW + 1], s_e2[BW + 1];
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) {
+  return __shfl_up_sync(0xffffffffu, v, 1);
+}
+template <typename T>
+__device__ __forceinline__ T shfl_down1(T v) {
+  return __shfl_down_sync(0xffffffffu, v, 1);
+}
+
+constexpr int kStripCols = 30;  // interior columns per warp strip
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                     const T* __restrict__ z, const T* __restrict__ n2,
+                                                     const int32_t* __restrict__ zone, const T* __restrict__ rates,
+                                                     int rows, int cols, int rb, T dx, T hextra) {
   if (!clk->active) return;
   const int src = clk->src, dst = clk->dst;
   const T dt = T(clk->global_dt);
@@ -187,101 +204,108 @@ __global__ void __launch_bounds__(BW) k_flux_update(const DevClock* __restrict__
   T* __restrict__ qxo = sb.qx[dst];
   T* __restrict__ qyo = sb.qy[dst];
 
-  const int t = threadIdx.x;
-  const int c0 = 1 + blockIdx.x * (BW - 2);
-  const int c = c0 - 1 + t;
-  const int r0 = 1 + blockIdx.y * rb;
-  const int r1 = min(r0 + rb - 1, rows - 2);
-  const bool incol = c < cols;
-  const bool mid = (t >= 1 && t <= BW - 2);
-  const bool upd = mid && c >= 1 && c <= cols - 2;
-  const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this thread
+  const int lane = threadIdx.x & 31;
+  const int nstrips = (cols - 2 + kStripCols - 1) / kStripCols;
+  const int nrowb = (rows - 2 + rb - 1) / rb;
+  const unsigned ntiles = (unsigned)nstrips * (unsigned)nrowb;
 
-  auto load = [&](int r) -> CellQ<T> {
-    CellQ<T> q;
-    if (incol) {
+  while (true) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(&clk->tile_next, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= ntiles) break;
+    const int sx = (int)(tile % nstrips), ry = (int)(tile / nstrips);
+    const int c = sx * kStripCols + lane;  // = c0 - 1 + lane with c0 = 1 + 30*sx
+    const int r0 = 1 + ry * rb;
+    const int r1 = min(r0 + rb - 1, rows - 2);
+    const bool incol = c < cols;
+    const bool mid = (lane >= 1 && lane <= kStripCols);
+    const bool upd = mid && c >= 1 && c <= cols - 2;
+    const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this lane
+    const bool owner = incol && (mid || gcol);
+
+    auto copy_ghost = [&](int r) {
       const size_t id = (size_t)r * cols + c;
-      q = make_cell<T>(hi[id], qxi[id], qyi[id], z[id], hextra);
-    } else {
-      q.h = q.qx = q.qy = q.z = q.sq = q.u = q.v = T(0);
-    }
-    return q;
-  };
-  auto copy_ghost = [&](int r) {
-    const size_t id = (size_t)r * cols + c;
-    ho[id] = hi[id];
-    qxo[id] = qxi[id];
-    qyo[id] = qyi[id];
-  };
+      ho[id] = hi[id];
+      qxo[id] = qxi[id];
+      qyo[id] = qyi[id];
+    };
 
-  CellQ<T> prev = load(r0 - 1);
-  if (r0 - 1 == 0 && incol && (mid || gcol)) copy_ghost(0);
-  RowParts<T> pp;
-  pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
-
-  for (int r = r0; r <= r1 + 1; ++r) {
-    const CellQ<T> cur = load(r);
-    FaceOut<T> Y;
-    Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
-    if (upd) Y = face_flux<T, false>(cur, prev, dx, dt, hextra);
-    if (r - 1 >= r0 && upd) {
-      const size_t id = (size_t)(r - 1) * cols + c;
-      T hn, qn, vn;
-      update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, n2[id], dt, hextra, hn, qn, vn);
-      if (nroff > 0) {  // update_runoff (kernels.h:128-149)
-        const T net = rates[(size_t)zone[id] * roff_rows + roff_row];
-        hn += net * dt;
-        if (hn < hextra) {
-          if (hn < T(0)) hn = T(0);
-          qn = T(0);
-          vn = T(0);
-        }
+    // raw values of the next row are loaded one iteration ahead
+    T lh = T(0), lqx = T(0), lqy = T(0), lz = T(0);
+    auto fetch = [&](int r) {
+      if (incol) {
+        const size_t id = (size_t)r * cols + c;
+        lh = hi[id];
+        lqx = qxi[id];
+        lqy = qyi[id];
+        lz = z[id];
       }
-      ho[id] = hn;
-      qxo[id] = qn;
-      qyo[id] = vn;
-    }
-    if (r > r1) {
-      if (r == rows - 1 && incol && (mid || gcol)) copy_ghost(r);
-      break;
-    }
-    // x faces of row r
-    s_h[t] = cur.h;
-    s_qx[t] = cur.qx;
-    s_qy[t] = cur.qy;
-    s_z[t] = cur.z;
-    s_sq[t] = cur.sq;
-    s_u[t] = cur.u;
-    s_v[t] = cur.v;
-    __syncthreads();
-    FaceOut<T> X;
-    X.a0 = X.a1 = X.a2 = X.b0 = X.b1 = X.b2 = T(0);
-    if (t >= 1 && incol && c >= 1) {
+    };
+    fetch(r0 - 1);
+    CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra);
+    if (r0 - 1 == 0 && owner) copy_ghost(0);
+    fetch(r0);
+    RowParts<T> pp;
+    pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
+    T pn2 = T(0);  // Manning of the previous row's cell
+
+    for (int r = r0; r <= r1 + 1; ++r) {
+      const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra);
+      T cn2 = T(0);
+      if (r <= r1) {
+        if (upd) cn2 = n2[(size_t)r * cols + c];
+        fetch(r + 1);  // r1 + 1 <= rows - 1
+      }
+      FaceOut<T> Y;
+      Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
+      if (upd) Y = face_flux<T, false>(cur, prev, dx, dt, hextra);
+      if (r - 1 >= r0 && upd) {
+        const size_t id = (size_t)(r - 1) * cols + c;
+        T hn, qn, vn;
+        update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn);
+        if (nroff > 0) {  // update_runoff (kernels.h:128-149)
+          const T net = rates[(size_t)zone[id] * roff_rows + roff_row];
+          hn += net * dt;
+          if (hn < hextra) {
+            if (hn < T(0)) hn = T(0);
+            qn = T(0);
+            vn = T(0);
+          }
+        }
+        ho[id] = hn;
+        qxo[id] = qn;
+        qyo[id] = vn;
+      }
+      if (r > r1) {
+        if (r == rows - 1 && owner) copy_ghost(r);
+        break;
+      }
+      // x faces of row r: lane l evaluates the face between lanes l-1 and l
       CellQ<T> left;
-      left.h = s_h[t - 1];
-      left.qx = s_qx[t - 1];
-      left.qy = s_qy[t - 1];
-      left.z = s_z[t - 1];
-      left.sq = s_sq[t - 1];
-      left.u = s_u[t - 1];
-      left.v = s_v[t - 1];
-      X = face_flux<T, true>(left, cur, dx, dt, hextra);
+      left.h = shfl_up1(cur.h);
+      left.qx = shfl_up1(cur.qx);
+      left.qy = shfl_up1(cur.qy);
+      left.z = shfl_up1(cur.z);
+      left.sq = shfl_up1(cur.sq);
+      left.u = shfl_up1(cur.u);
+      left.v = shfl_up1(cur.v);
+      FaceOut<T> X;
+      X.a0 = X.a1 = X.a2 = X.b0 = X.b1 = X.b2 = T(0);
+      if (lane >= 1 && incol && c >= 1) X = face_flux<T, true>(left, cur, dx, dt, hextra);
+      pp.e0 = shfl_down1(X.a0);
+      pp.e1 = shfl_down1(X.a1);
+      pp.e2 = shfl_down1(X.a2);
+      pp.w0 = X.b0;
+      pp.w1 = X.b1;
+      pp.w2 = X.b2;
+      pp.n0 = Y.a0;
+      pp.n1 = Y.a1;
+      pp.n2 = Y.a2;
+      pn2 = cn2;
+      if (gcol) copy_ghost(r);
+      prev = cur;
     }
-    s_e0[t] = X.a0;
-    s_e1[t] = X.a1;
-    s_e2[t] = X.a2;
-    __syncthreads();
-    pp.e0 = s_e0[t + 1 < BW ? t + 1 : t];
-    pp.e1 = s_e1[t + 1 < BW ? t + 1 : t];
-    pp.e2 = s_e2[t + 1 < BW ? t + 1 : t];
-    pp.w0 = X.b0;
-    pp.w1 = X.b1;
-    pp.w2 = X.b2;
-    pp.n0 = Y.a0;
-    pp.n1 = Y.a1;
-    pp.n2 = Y.a2;
-    if (gcol) copy_ghost(r);
-    prev = cur;
   }
 }
 
