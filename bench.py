@@ -226,6 +226,7 @@ def main():
     d = sc.to_domain(args.precision, stream=stream.cuda_stream)
     # no events inside the measured steps: the loop never stops to print
     d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    tuning = d.autotune(trial_steps=8)
     n, _ = d.advance(args.warmup)
     assert n == args.warmup
     barrier()
@@ -309,7 +310,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": desc, "grid": [sc.rows - 2, sc.cols - 2], "interior_cells": cells,
                        "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state ~%d MB per GPU)" % (sc.rows * sc.cols * 72 // 2 ** 20)},
+                       "l2": "inputs larger than L2 (state ~%d MB per GPU)" % (sc.rows * sc.cols * 72 // 2 ** 20),
+                       "flux_launch_shape": tuning},
             "roofline": {"bound": "hbm", "kernel": "k_flux_update", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": (tpc * cells) if tpc is not None else None,

@@ -172,6 +172,25 @@ int tri_domain_set_timing(tri_domain* d, int32_t enabled);
 int tri_domain_get_timing(tri_domain* d, double* flux_ms, int32_t* flux_launches, double* wetdry_ms,
                           int32_t* wetdry_launches);
 
+/* Launch-shape autotuner of the flux kernel.  Runs trial_steps steps of the
+ * domain's own state for every candidate (register budget x tile height),
+ * keeps the fastest, and restores the state and clock, so the simulation is
+ * unchanged.  The choice stays with the domain. */
+typedef struct tri_tuning {
+  int32_t variant;        /* register-budget variant of the flux kernel */
+  int32_t rows_per_tile;  /* tile height (rows per warp tile, 30 columns wide) */
+  int32_t candidates;     /* how many shapes were timed */
+  int32_t flux_blocks;    /* blocks in the flux kernel's grid */
+  double ms_per_step;     /* best trial time per step */
+} tri_tuning;
+int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out);
+int tri_domain_get_tuning(tri_domain* d, tri_tuning* out);
+
+/* Self-check of the exact division by a reused divisor used in the kernels:
+ * n pseudo-random (a, b) pairs from 'seed' over the magnitudes the step
+ * produces; counts quotients that differ in any bit from IEEE a/b. */
+int tri_selftest_division(int64_t n, uint64_t seed, int64_t* mismatches);
+
 /* ---- reference kernels (FP64, device pointers) -------------------------- */
 /* Each launches on 'stream' (cudaStream_t, NULL = default stream) and does not
  * synchronize.  size/rows/cols as in the reference; 'stream' is added last. */

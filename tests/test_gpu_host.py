@@ -75,10 +75,10 @@ def test_synthetic_case_matches_reference_executable(tmp_path):
     from triton_b200 import scenarios
     sc = scenarios.mixed(rows=45, cols=71, seed=17, open_boundaries=0, friction=True, duration=12.0)
     outs = {}
+    cfg = scenarios.write_case(sc, str(tmp_path / "input"), fmt="BIN", output_format="ASC", max_value_print="h")
     for name, exe in (("ours", EXE), ("ref", REF)):
         base = tmp_path / name
-        cfg = scenarios.write_case(sc, str(base / "input"), fmt="BIN", output_format="ASC", max_value_print="h")
-        (base / "bin").mkdir()
+        (base / "bin").mkdir(parents=True)
         os.symlink(exe, base / "bin" / "triton.exe")
         _run(str(base / "bin" / "triton.exe"), base, cfg)
         outs[name] = base / "output"

@@ -67,3 +67,37 @@ def test_wide_grid_multiple_strips():
     from triton_b200 import scenarios
     sc = scenarios.mixed(rows=150, cols=300, seed=5, friction=False, with_extbc=False, duration=4.0)
     run_lockstep(sc, exact=True, check_every_event=False)
+
+
+def test_exact_division_selftest():
+    """The kernels divide by dx and dt through a correctly rounded reciprocal
+    and one Markstein correction; the quotient must equal IEEE a/b in every
+    bit over the operand ranges the step produces."""
+    import ctypes as C
+    from triton_b200 import _abi
+    bad = C.c_int64(-1)
+    _abi.check(_abi.lib().tri_selftest_division(50_000_000, 12345, C.byref(bad)))
+    assert bad.value == 0
+
+
+def test_autotune_keeps_state_and_parity():
+    from tests._harness import compare_fields, oracle_from_scenario, oracle_bookkeeping, domain_bookkeeping
+    from triton_b200 import scenarios
+    sc = scenarios.dambreak(n=120, dx=1.0, radius=25.0, depth=4.0, duration=2.0)
+    o = oracle_from_scenario(sc)
+    d = sc.to_domain()
+    try:
+        t = d.autotune(trial_steps=4)
+        assert t["candidates"] >= 3 and t["ms_per_step"] > 0
+        assert d.get_clock().it_count == 0
+        while True:
+            n1, e1 = o.advance(10 ** 6)
+            n2, e2 = d.advance(10 ** 6)
+            assert (n1, e1) == (n2, e2)
+            compare_fields(o, d, True, sc.hextra)
+            oracle_bookkeeping(o, e1)
+            domain_bookkeeping(d, e2)
+            if e1 & 1:
+                break
+    finally:
+        d.close()

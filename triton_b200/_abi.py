@@ -39,6 +39,11 @@ class Progress(C.Structure):
     _fields_ = [("steps", C.c_int32), ("events", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("rows_per_tile", C.c_int32), ("candidates", C.c_int32),
+                ("flux_blocks", C.c_int32), ("ms_per_step", C.c_double)]
+
+
 class TriError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"triton_b200 error {code}: {msg}")
@@ -67,6 +72,9 @@ _SIGS = {
     "tri_domain_synchronize": (C.c_int, [_vp]),
     "tri_domain_set_timing": (C.c_int, [_vp, C.c_int32]),
     "tri_domain_get_timing": (C.c_int, [_vp, _dp, _ip, _dp, _ip]),
+    "tri_domain_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
+    "tri_domain_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
+    "tri_selftest_division": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     "tri_kernel_compute_dt_and_sqrt_f64": (C.c_int, [C.c_int, C.c_double, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                                      C.c_double, _vp]),
     "tri_kernel_find_min_dt_f64": (C.c_int, [C.c_int, _vp, _vp, _vp]),

@@ -31,6 +31,24 @@ __device__ __forceinline__ float dev_fmax(float a, float b) { return fmaxf(a, b)
 __device__ __forceinline__ double dev_fmin(double a, double b) { return fmin(a, b); }
 __device__ __forceinline__ float dev_fmin(float a, float b) { return fminf(a, b); }
 
+__device__ __forceinline__ double dev_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float dev_fma(float a, float b, float c) { return fmaf(a, b, c); }
+
+// a / b rounded to nearest from y = RN(1/b), the correctly rounded reciprocal
+// (Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990): q0 = RN(a*y) is within
+// one ulp of a/b, the residual r = a - b*q0 is exact in one fused
+// multiply-add, and RN(q0 + r*y) is the correctly rounded quotient.  The
+// theorem needs a, b and a/b normal (no overflow or underflow).  An exact
+// quotient (r == 0) returns q0 itself, which also keeps the sign of a zero.
+// Three operations instead of a full division when the divisor is reused.
+template <typename T>
+__device__ __forceinline__ T div_by_rcp(T a, T b, T y) {
+  const T q0 = a * y;
+  const T r = dev_fma(-q0, b, a);
+  return r == T(0) ? q0 : dev_fma(r, y, q0);
+}
+
 // Order-preserving key of a non-negative double for an unsigned atomic min.
 // NaN maps to +inf so it is never the minimum (the reference's
 // "a < m ? a : m" fold never selects a NaN either).

@@ -112,8 +112,9 @@ struct tri_domain {
   double* vol_part = nullptr;
   double* vol_out = nullptr;
   int vol_blocks = 0;
-  // launch shape of the flux kernel
-  int rb = 16, flux_blocks = 1;
+  // launch shape of the flux kernel (tile height, register variant, grid)
+  int rb = 16, flux_blocks = 1, flux_variant = 0;
+  double tuned_ms = 0;
   // graphs of 'graph_steps' steps
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -210,26 +211,64 @@ __global__ void k_volume_sum(const double* __restrict__ part, int n, double scal
   *out = acc * scale;
 }
 
+// Register-budget variants of the flux kernel: at least 3, 4 or 5 resident
+// 128-thread blocks per SM (fewer registers per thread, more warps to hide
+// FP64 latency).  The autotuner picks one per domain.
+constexpr int kFluxVariants = 3;
+constexpr int kFluxMinBlocks[kFluxVariants] = {3, 4, 5};
+
+template <typename T>
+void flux_occupancy(int variant, int* per_sm) {
+  switch (variant) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 3>, 128, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 4>, 128, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 5>, 128, 0); break;
+  }
+}
+
+template <typename T>
+void launch_flux(tri_domain* d, StateBufs<T> sb, T dx, T hx) {
+  const int rows = d->desc.rows, cols = d->desc.cols;
+  const T rdx = (T)(1.0 / d->desc.cell_size);
+#define TRI_FLUX_ARGS                                                                                          \
+  d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone, (const T*)d->rates, rows, cols, d->rb, dx, rdx, hx
+  switch (d->flux_variant) {
+    case 0: k_flux_update<T, 3><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
+    case 1: k_flux_update<T, 4><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
+    default: k_flux_update<T, 5><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
+  }
+#undef TRI_FLUX_ARGS
+}
+
+// Grid of the flux kernel for the domain's variant and tile height: one
+// resident wave of blocks, each warp fetching tiles until none are left.
+void size_flux_grid(tri_domain* d) {
+  const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int per_sm = 0;
+  if (d->prec == TRI_FP64)
+    flux_occupancy<double>(d->flux_variant, &per_sm);
+  else
+    flux_occupancy<float>(d->flux_variant, &per_sm);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t strips = (cols + kStripCols - 1) / kStripCols;
+  const int64_t tiles = strips * ((rows + d->rb - 1) / d->rb);
+  d->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
+}
+
+// Default shape before any tuning: the largest tile height that still gives
+// every warp of a full wave about eight tiles.
 void choose_shape(tri_domain* d) {
-  // Tiles of 30 columns x rb rows, one warp each, fetched dynamically by a
-  // grid that fills every SM once; short tiles waste halo rows, too few
-  // tiles leave warps without work at the end of a step.
   const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
   int sms = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t strips = (cols + kStripCols - 1) / kStripCols;
-  int per_sm = 0;
-  if (d->prec == TRI_FP64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flux_update<double>, 128, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flux_update<float>, 128, 0);
-  if (per_sm < 1) per_sm = 1;
-  const int64_t warps = (int64_t)sms * per_sm * 4;
+  const int64_t warps = (int64_t)sms * 12;
   int rb = 32;
   while (rb > 4 && strips * ((rows + rb - 1) / rb) < 8 * warps) rb /= 2;
   d->rb = rb;
-  const int64_t tiles = strips * ((rows + rb - 1) / rb);
-  d->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
+  size_flux_grid(d);
 }
 
 template <typename T>
@@ -249,8 +288,7 @@ int launch_step(tri_domain* d) {
     d->tev_used += 4;
     cudaEventRecord(ev[0], d->stream);
   }
-  k_flux_update<T><<<d->flux_blocks, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone,
-                                                          (const T*)d->rates, rows, cols, d->rb, dx, hx);
+  launch_flux<T>(d, sb, dx, hx);
   if (ev) cudaEventRecord(ev[1], d->stream);
   if (d->nsrc > 0) {
     for (size_t w = 0; w + 1 < d->src_waves.size(); w++) {
@@ -806,6 +844,98 @@ int tri_domain_volume(tri_domain* d, double* volume) {
   TRI_CUDA_TRY(cudaGetLastError());
   TRI_CUDA_TRY(cudaMemcpyAsync(volume, d->vol_out, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out) {
+  TRI_CHECK_ARG(d && out, "null argument");
+  TRI_CHECK_ARG(trial_steps >= 1, "trial_steps must be >= 1");
+  DevClock* m = d->mirror;
+  const DevClock saved = *m;
+  const bool saved_valid = d->dt_valid;
+  const int cur = m->cur;
+  const size_t fb = d->ncells * d->esize;
+  // back up the current state and max depth
+  void* bak = nullptr;
+  TRI_CUDA_TRY(cudaMalloc(&bak, 4 * fb));
+  char* b = (char*)bak;
+  auto save_restore = [&](bool save) -> int {
+    void* f[4] = {d->h[cur], d->qx[cur], d->qy[cur], d->maxh};
+    for (int i = 0; i < 4; i++) {
+      if (save)
+        TRI_CUDA_TRY(cudaMemcpyAsync(b + i * fb, f[i], fb, cudaMemcpyDeviceToDevice, d->stream));
+      else
+        TRI_CUDA_TRY(cudaMemcpyAsync(f[i], b + i * fb, fb, cudaMemcpyDeviceToDevice, d->stream));
+    }
+    return TRI_OK;
+  };
+  int rc = save_restore(true);
+  const int heights[3] = {8, 16, 32};
+  double best = 1e300;
+  int best_v = d->flux_variant, best_rb = d->rb, ncand = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const bool timing = d->timing;
+  d->timing = false;
+  for (int v = 0; v < kFluxVariants && rc == TRI_OK; v++) {
+    for (int hi = 0; hi < 3 && rc == TRI_OK; hi++) {
+      if (heights[hi] > std::max(8, d->desc.rows - 2)) continue;
+      d->flux_variant = v;
+      d->rb = heights[hi];
+      size_flux_grid(d);
+      drop_graph(d);
+      rc = save_restore(false);
+      if (rc != TRI_OK) break;
+      *m = saved;
+      m->sim_duration = m->print_interval = m->print_observation = 1e300;
+      m->it_print = 0;
+      m->time_series = 0;
+      m->halt = 0;
+      m->dt_key[m->rd] = kDtKeyInf;
+      rc = push_clock(d);
+      if (rc == TRI_OK) rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+      if (rc == TRI_OK) rc = launch_steps(d, 2);  // warm-up (also builds the graph)
+      cudaEventRecord(e0, d->stream);
+      if (rc == TRI_OK) rc = launch_steps(d, trial_steps);
+      cudaEventRecord(e1, d->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = set_error(TRI_E_CUDA, "autotune trial failed");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ncand++;
+      if (rc == TRI_OK && ms / trial_steps < best) {
+        best = ms / trial_steps;
+        best_v = v;
+        best_rb = heights[hi];
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  d->timing = timing;
+  d->flux_variant = best_v;
+  d->rb = best_rb;
+  size_flux_grid(d);
+  drop_graph(d);
+  int rc2 = save_restore(false);
+  *m = saved;
+  d->dt_valid = saved_valid;
+  if (rc2 == TRI_OK) rc2 = push_clock(d);
+  cudaStreamSynchronize(d->stream);
+  cudaFree(bak);
+  if (rc != TRI_OK) return rc;
+  if (rc2 != TRI_OK) return rc2;
+  d->tuned_ms = best;
+  return tri_domain_get_tuning(d, out);
+}
+
+int tri_domain_get_tuning(tri_domain* d, tri_tuning* out) {
+  TRI_CHECK_ARG(d && out, "null argument");
+  out->variant = d->flux_variant;
+  out->rows_per_tile = d->rb;
+  out->candidates = kFluxVariants * 3;
+  out->flux_blocks = d->flux_blocks;
+  out->ms_per_step = d->tuned_ms;
   return TRI_OK;
 }
 

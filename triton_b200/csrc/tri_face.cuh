@@ -50,8 +50,16 @@ struct FaceOut {
   T a0, a1, a2, b0, b1, b2;
 };
 
+// Step constants of the face solver: rdx = RN(1/dx) and rdt = RN(1/dt) turn
+// the divisions by dx and dt into exact three-operation quotients.
+template <typename T>
+struct StepK {
+  T dx, dt, rdx, rdt, hextra;
+};
+
 template <typename T, bool XFACE>
-__device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<T>& c2, T dx, T dt, T hextra) {
+__device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<T>& c2, const StepK<T>& K) {
+  const T dx = K.dx, dt = K.dt, hextra = K.hextra;
   constexpr T nx = XFACE ? T(1) : T(0);
   constexpr T ny = XFACE ? T(0) : T(1);
   const T G = T(kGravity), SG = T(kSqrtG), E12 = eps12<T>();
@@ -117,8 +125,8 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   // positivity limiter on subcritical wet-wet faces
   hp = h1 + al0;
   if (lam0 * lam2 < T(0) && hp > T(0) && h1 > T(0) && h2 > T(0)) {
-    be0 = dev_fmax(be0, lam0 / (lam0 + lamE2) * (al0 * lam0 - h1 * dx * T(0.5) / dt + lamE2 * h2));
-    be0 = dev_fmin(be0, lam2 / (lam2 + lamE0) * (-al2 * lam2 + h2 * dx * T(0.5) / dt + lamE0 * h1));
+    be0 = dev_fmax(be0, lam0 / (lam0 + lamE2) * (al0 * lam0 - div_by_rcp(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
+    be0 = dev_fmin(be0, lam2 / (lam2 + lamE0) * (-al2 * lam2 + div_by_rcp(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
   }
   const T be2 = -be0;
   const T be1 = T(0);
@@ -212,12 +220,12 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   if (dev_fabs(q1) < E12) q1 = T(0);
   if (dev_fabs(p2) < E12) p2 = T(0);
   if (dev_fabs(q2) < E12) q2 = T(0);
-  out.a0 = dt * p0 / dx;
-  out.a1 = dt * p1 / dx;
-  out.a2 = dt * p2 / dx;
-  out.b0 = dt * q0 / dx;
-  out.b1 = dt * q1 / dx;
-  out.b2 = dt * q2 / dx;
+  out.a0 = div_by_rcp(dt * p0, dx, K.rdx);
+  out.a1 = div_by_rcp(dt * p1, dx, K.rdx);
+  out.a2 = div_by_rcp(dt * p2, dx, K.rdx);
+  out.b0 = div_by_rcp(dt * q0, dx, K.rdx);
+  out.b1 = div_by_rcp(dt * q1, dx, K.rdx);
+  out.b2 = div_by_rcp(dt * q2, dx, K.rdx);
   return out;
 }
 

@@ -27,6 +27,7 @@ struct DevClock {
   double simtime, sim_duration, print_interval, print_observation, last_obs_time;
   double init_dt, time_step, average_dt, global_dt;
   double t_step;  // simtime at the start of the running step
+  double rdt;     // RN(1/global_dt)
   int32_t print_id, it_count, it_print, time_series, time_increment_fixed;
   int32_t runoff_row, src_idx_low, src_idx_high;
   int32_t active, halt, events, steps;
@@ -69,6 +70,7 @@ __global__ void k_clock(DevClock* __restrict__ c) {
     dt = c->time_step;
   }
   c->global_dt = dt;
+  c->rdt = 1.0 / dt;
   c->t_step = t0;
   c->it_count++;
   if (c->nroff > 0) {
@@ -188,14 +190,20 @@ __device__ __forceinline__ T shfl_down1(T v) {
 
 constexpr int kStripCols = 30;  // interior columns per warp strip
 
-template <typename T>
-__global__ void __launch_bounds__(128) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                      const T* __restrict__ z, const T* __restrict__ n2,
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
-                                                     int rows, int cols, int rb, T dx, T hextra) {
+                                                     int rows, int cols, int rb, T dx, T rdx, T hextra) {
   if (!clk->active) return;
   const int src = clk->src, dst = clk->dst;
   const T dt = T(clk->global_dt);
+  StepK<T> K;
+  K.dx = dx;
+  K.dt = dt;
+  K.rdx = rdx;
+  K.rdt = T(clk->rdt);
+  K.hextra = hextra;
   const int nroff = clk->nroff, roff_rows = clk->roff_rows, roff_row = clk->runoff_row;
   const T* __restrict__ hi = sb.h[src];
   const T* __restrict__ qxi = sb.qx[src];
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(128) k_flux_update(DevClock* __restrict__ clk,
       }
       FaceOut<T> Y;
       Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
-      if (upd) Y = face_flux<T, false>(cur, prev, dx, dt, hextra);
+      if (upd) Y = face_flux<T, false>(cur, prev, K);
       if (r - 1 >= r0 && upd) {
         const size_t id = (size_t)(r - 1) * cols + c;
         T hn, qn, vn;
@@ -292,7 +300,7 @@ __global__ void __launch_bounds__(128) k_flux_update(DevClock* __restrict__ clk,
       left.v = shfl_up1(cur.v);
       FaceOut<T> X;
       X.a0 = X.a1 = X.a2 = X.b0 = X.b1 = X.b2 = T(0);
-      if (lane >= 1 && incol && c >= 1) X = face_flux<T, true>(left, cur, dx, dt, hextra);
+      if (lane >= 1 && incol && c >= 1) X = face_flux<T, true>(left, cur, K);
       pp.e0 = shfl_down1(X.a0);
       pp.e1 = shfl_down1(X.a1);
       pp.e2 = shfl_down1(X.a2);

@@ -161,6 +161,14 @@ class Domain:
         check(lib().tri_domain_get_timing(self._h, C.byref(a), C.byref(na), C.byref(b), C.byref(nb)))
         return a.value, na.value, b.value, nb.value
 
+    def autotune(self, trial_steps=10):
+        """Times every flux-kernel launch shape on this domain's own state and
+        keeps the fastest; the state and clock are restored afterwards."""
+        t = _abi.Tuning()
+        check(lib().tri_domain_autotune(self._h, int(trial_steps), C.byref(t)))
+        return dict(variant=t.variant, rows_per_tile=t.rows_per_tile, candidates=t.candidates,
+                    flux_blocks=t.flux_blocks, ms_per_step=t.ms_per_step)
+
     def run(self, on_event=None, max_chunk=1 << 30):
         """Run to sim_duration reacting to events like triton_simulate.h:54-134.
 
