@@ -195,6 +195,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="grid side (default: the workload's full size)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="", help="flux kernel launch shape 'variant:rows_per_tile' (skips autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -226,7 +227,12 @@ def main():
     d = sc.to_domain(args.precision, stream=stream.cuda_stream)
     # no events inside the measured steps: the loop never stops to print
     d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
-    tuning = d.autotune(trial_steps=8)
+    if args.shape:
+        v, rb = (int(x) for x in args.shape.split(":"))
+        d.set_shape(v, rb)
+        tuning = {"variant": v, "rows_per_tile": rb, "source": "--shape"}
+    else:
+        tuning = d.autotune(trial_steps=8)
     n, _ = d.advance(args.warmup)
     assert n == args.warmup
     barrier()

@@ -185,6 +185,8 @@ typedef struct tri_tuning {
 } tri_tuning;
 int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out);
 int tri_domain_get_tuning(tri_domain* d, tri_tuning* out);
+/* Sets the flux kernel's launch shape directly (variant 0..2, rows per tile >= 1). */
+int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile);
 
 /* Self-check of the exact division by a reused divisor used in the kernels:
  * n pseudo-random (a, b) pairs from 'seed' over the magnitudes the step

@@ -939,6 +939,18 @@ int tri_domain_get_tuning(tri_domain* d, tri_tuning* out) {
   return TRI_OK;
 }
 
+int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CHECK_ARG(variant >= 0 && variant < kFluxVariants, "variant %d outside [0,%d)", variant, kFluxVariants);
+  TRI_CHECK_ARG(rows_per_tile >= 1, "rows_per_tile must be >= 1");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->flux_variant = variant;
+  d->rb = rows_per_tile;
+  size_flux_grid(d);
+  drop_graph(d);
+  return TRI_OK;
+}
+
 int tri_domain_synchronize(tri_domain* d) {
   TRI_CHECK_ARG(d, "null domain");
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));

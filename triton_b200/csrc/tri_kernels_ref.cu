@@ -36,10 +36,15 @@ __global__ void kr_compute_dt_and_sqrt(int size, double dx, const double* __rest
 // reduction of order-preserving keys and one atomicMin per block.  The first
 // block seeds the result with +inf before any block folds into it (a flag word
 // next to the result is not available, so the seed is a separate launch).
-__global__ void kr_seed_min(unsigned long long* out) { *out = kDtKeyInf; }
+// Keys of this path order every double (negatives included): positive values
+// get the sign bit set, negative ones are complemented.  The empty key is the
+// largest one.
+constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+
+__global__ void kr_seed_min(unsigned long long* out) { *out = kEmptyKey; }
 
 __global__ void kr_min_keys(int size, const double* __restrict__ v, unsigned long long* __restrict__ out) {
-  unsigned long long key = kDtKeyInf;
+  unsigned long long key = kEmptyKey;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
     const double x = v[i];
     // The reference folds with "a < m ? a : m" from the largest double, so
@@ -47,7 +52,7 @@ __global__ void kr_min_keys(int size, const double* __restrict__ v, unsigned lon
     // matches the numeric one.
     unsigned long long k;
     if (x != x) {
-      k = kDtKeyInf;
+      k = kEmptyKey;
     } else {
       const unsigned long long b = (unsigned long long)__double_as_longlong(x);
       k = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
@@ -64,7 +69,7 @@ __global__ void kr_min_keys(int size, const double* __restrict__ v, unsigned lon
   if (lane == 0) s[warp] = key;
   __syncthreads();
   if (warp == 0) {
-    key = lane < (int)(blockDim.x >> 5) ? s[lane] : kDtKeyInf;
+    key = lane < (int)(blockDim.x >> 5) ? s[lane] : kEmptyKey;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
@@ -79,7 +84,7 @@ __global__ void kr_decode_min(unsigned long long* slot) {
   // largest double, as Kokkos::Min starts from it)
   const unsigned long long k = *slot;
   double v;
-  if (k == kDtKeyInf) {
+  if (k == kEmptyKey) {
     v = 1.7976931348623157e308;
   } else {
     const unsigned long long b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;

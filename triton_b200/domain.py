@@ -169,6 +169,9 @@ class Domain:
         return dict(variant=t.variant, rows_per_tile=t.rows_per_tile, candidates=t.candidates,
                     flux_blocks=t.flux_blocks, ms_per_step=t.ms_per_step)
 
+    def set_shape(self, variant, rows_per_tile):
+        check(lib().tri_domain_set_tuning(self._h, int(variant), int(rows_per_tile)))
+
     def run(self, on_event=None, max_chunk=1 << 30):
         """Run to sim_duration reacting to events like triton_simulate.h:54-134.
 
