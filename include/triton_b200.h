@@ -165,6 +165,16 @@ int tri_domain_observe(tri_domain* d, double* h, double* qx, double* qy);
 /* Sum of h over interior cells times dx^2, accumulated in FP64. */
 int tri_domain_volume(tri_domain* d, double* volume);
 int tri_domain_synchronize(tri_domain* d);
+/* Volume accounts (FP32 form; zeros in the FP64 form), m^3: out[0] interior
+ * volume now (FP64 sum), then the cumulative Kahan-compensated FP64 totals of
+ * inflow through boundary faces, point sources, runoff, external-boundary
+ * depth resets and negative-depth clipping since the last H upload.  Volume
+ * conservation: out[0] - V0 == out[1] + ... + out[5]. */
+int tri_domain_mass_balance(tri_domain* d, double* out6);
+/* Records, per cell, the first simtime at which h exceeds 'depth' (arrival
+ * time); download gives -1 for cells never reached. */
+int tri_domain_track_arrival(tri_domain* d, double depth);
+int tri_domain_download_arrival(tri_domain* d, double* host, int64_t n);
 /* Kernel timing with CUDA events on the domain's stream: when enabled,
  * advance() records the flux/update kernel and the wet-dry/dt kernel.
  * Reports total milliseconds and launch counts since the last reset. */
@@ -224,8 +234,10 @@ int tri_kernel_copy_info_to_exterior_boundaries_west_east_f64(int size, int nrow
 int tri_kernel_copy_info_to_exterior_boundaries_north_south_f64(int size, int nrows, int ncols, double* h,
                                                                 double* qx, double* qy, int rank,
                                                                 int total_process, void* stream);
-/* compute_extbc_values: cells are applied in index order where two of them
- * touch the same cell (corners shared by two segments). */
+/* compute_extbc_values: cells that touch the same cell (corners shared by two
+ * segments, repeated cells) are applied in index order, as the reference's
+ * serial build does; to schedule them the entry reads the cell list back to
+ * the host, so it synchronizes 'stream'. */
 int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy,
                                         const double* dem, const double* n, const int32_t* relative_index,
                                         const int32_t* extbctype, const int32_t* start_index,

@@ -70,6 +70,9 @@ _SIGS = {
     "tri_domain_observe": (C.c_int, [_vp, _dp, _dp, _dp]),
     "tri_domain_volume": (C.c_int, [_vp, _dp]),
     "tri_domain_synchronize": (C.c_int, [_vp]),
+    "tri_domain_mass_balance": (C.c_int, [_vp, _dp]),
+    "tri_domain_track_arrival": (C.c_int, [_vp, C.c_double]),
+    "tri_domain_download_arrival": (C.c_int, [_vp, _dp, C.c_int64]),
     "tri_domain_set_timing": (C.c_int, [_vp, C.c_int32]),
     "tri_domain_get_timing": (C.c_int, [_vp, _dp, _ip, _dp, _ip]),
     "tri_domain_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),

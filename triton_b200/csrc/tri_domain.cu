@@ -34,10 +34,7 @@ int set_error(int code, const char* fmt, ...) {
   return code;
 }
 
-// Conflict-free waves: item k goes one wave after the latest earlier item
-// that touches one of its cells, so items sharing a cell keep their index
-// order and all others run in parallel.
-static void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<int32_t>& order,
+void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<int32_t>& order,
                         std::vector<int32_t>& wave_start) {
   const int n = (int)touches.size();
   std::map<int64_t, int> last;
@@ -81,6 +78,10 @@ struct tri_domain {
   void* n2 = nullptr;
   void* maxh = nullptr;
   double* stage = nullptr;  // FP64 staging field for FP32 uploads/downloads
+  double* zbase = nullptr;  // FP32 form: FP64 bed base level per 32x32 tile
+  int ntc = 0, ntr = 0;     // tiles per row / per column
+  float* arrival = nullptr; // optional first time h exceeds arrival_depth
+  float arrival_depth = 0.1f;
   // runoff
   int32_t nroff = 0, roff_rows = 0;
   int32_t* zone = nullptr;
@@ -140,6 +141,17 @@ StateBufs<T> bufs(tri_domain* d) {
   return s;
 }
 
+constexpr int kWetBand = 16;  // rows per block of the wet-dry/dt kernel
+
+template <typename T>
+BedMap<T> bedmap(tri_domain* d) {
+  BedMap<T> b;
+  b.z = (const T*)d->z;
+  b.base = d->zbase;
+  b.ntc = d->ntc;
+  return b;
+}
+
 void free_dev(void*& p) {
   if (p) cudaFree(p);
   p = nullptr;
@@ -172,6 +184,22 @@ template <typename T>
 __global__ void k_to_f64(const T* __restrict__ src, double* __restrict__ dst, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[i] = (double)src[i];
+}
+
+// FP32 form: offsets of the bed from each 32x32 tile's FP64 base level.
+__global__ void k_bed_offsets(const double* __restrict__ z, const double* __restrict__ base, float* __restrict__ off,
+                              int rows, int cols, int ntc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)rows * cols) return;
+  const int r = (int)(i / cols), c = (int)(i % cols);
+  off[i] = (float)(z[i] - base[(r >> 5) * ntc + (c >> 5)]);
+}
+__global__ void k_bed_levels(const float* __restrict__ off, const double* __restrict__ base, double* __restrict__ z,
+                             int rows, int cols, int ntc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)rows * cols) return;
+  const int r = (int)(i / cols), c = (int)(i % cols);
+  z[i] = base[(r >> 5) * ntc + (c >> 5)] + (double)off[i];
 }
 
 template <typename T>
@@ -231,7 +259,7 @@ void launch_flux(tri_domain* d, StateBufs<T> sb, T dx, T hx) {
   const int rows = d->desc.rows, cols = d->desc.cols;
   const T rdx = (T)(1.0 / d->desc.cell_size);
 #define TRI_FLUX_ARGS                                                                                          \
-  d->clk, sb, (const T*)d->z, (const T*)d->n2, d->zone, (const T*)d->rates, rows, cols, d->rb, dx, rdx, hx
+  d->clk, sb, bedmap<T>(d), (const T*)d->n2, d->zone, (const T*)d->rates, rows, cols, d->rb, dx, rdx, hx
   switch (d->flux_variant) {
     case 0: k_flux_update<T, 3><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
     case 1: k_flux_update<T, 4><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
@@ -304,15 +332,17 @@ int launch_step(tri_domain* d) {
   if (d->nbc > 0) {
     for (size_t w = 0; w + 1 < d->bc_waves.size(); w++) {
       const int off = d->bc_waves[w], cnt = d->bc_waves[w + 1] - off;
-      k_extbc<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (const T*)d->n2,
+      k_extbc<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, bedmap<T>(d), (const T*)d->n2,
                                                            d->bc_order + off, cnt, d->bc_cells, d->bc_types,
                                                            d->bc_start, d->bc_nrows, (const T*)d->bc_v1,
                                                            (const T*)d->bc_v2, rows, cols);
     }
   }
-  dim3 b2(32, 8), g2((cols + 31) / 32, (rows + 7) / 8);
+  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
   if (ev) cudaEventRecord(ev[2], d->stream);
-  k_wetdry_dt<T, true><<<g2, b2, 0, d->stream>>>(d->clk, sb, (const T*)d->z, (T*)d->maxh, rows, cols, dx, cn, hx);
+  k_wetdry_dt<T, true><<<g2, kWetCols, 0, d->stream>>>(d->clk, sb, bedmap<T>(d), (T*)d->maxh, rows, cols,
+                                                       kWetBand, d->desc.cell_size, d->desc.courant, hx,
+                                                       d->arrival, d->arrival_depth);
   if (ev) cudaEventRecord(ev[3], d->stream);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;
@@ -321,9 +351,10 @@ int launch_step(tri_domain* d) {
 template <typename T>
 int launch_initial_dt(tri_domain* d) {
   const int rows = d->desc.rows, cols = d->desc.cols;
-  dim3 b2(32, 8), g2((cols + 31) / 32, (rows + 7) / 8);
-  k_wetdry_dt<T, false><<<g2, b2, 0, d->stream>>>(d->clk, bufs<T>(d), (const T*)d->z, (T*)d->maxh, rows, cols,
-                                                  (T)d->desc.cell_size, (T)d->desc.courant, (T)d->desc.hextra);
+  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
+  k_wetdry_dt<T, false><<<g2, kWetCols, 0, d->stream>>>(d->clk, bufs<T>(d), bedmap<T>(d), (T*)d->maxh, rows,
+                                                        cols, kWetBand, d->desc.cell_size, d->desc.courant,
+                                                        (T)d->desc.hextra, nullptr, 0.0f);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;
 }
@@ -453,9 +484,13 @@ int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out)
                             cudaGetErrorString(e)));
     cudaMemsetAsync(*f, 0, fb, d->stream);
   }
+  d->ntr = (desc->rows + 31) / 32;
+  d->ntc = (desc->cols + 31) / 32;
   if (d->prec == TRI_FP32) {
-    if (cudaMalloc((void**)&d->stage, d->ncells * 8) != cudaSuccess)
+    if (cudaMalloc((void**)&d->stage, d->ncells * 8) != cudaSuccess ||
+        cudaMalloc((void**)&d->zbase, (size_t)d->ntr * d->ntc * 8) != cudaSuccess)
       return fail(set_error(TRI_E_NOMEM, "cudaMalloc staging field failed"));
+    cudaMemsetAsync(d->zbase, 0, (size_t)d->ntr * d->ntc * 8, d->stream);
   }
   if (cudaMalloc((void**)&d->clk, sizeof(DevClock)) != cudaSuccess ||
       cudaMallocHost((void**)&d->mirror, sizeof(DevClock)) != cudaSuccess ||
@@ -494,6 +529,8 @@ int tri_domain_destroy(tri_domain* d) {
   free_dev(d->n2);
   free_dev(d->maxh);
   free_devp(d->stage);
+  free_devp(d->zbase);
+  free_devp(d->arrival);
   free_devp(d->zone);
   free_dev(d->rates);
   free_devp(d->roff_t);
@@ -532,6 +569,20 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   if (rc != TRI_OK) return rc;
   if (d->prec == TRI_FP64) {
     TRI_CUDA_TRY(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+  } else if (field == TRI_FIELD_DEM) {
+    // base level of each 32x32 tile = its lowest cell (below the 1e6 walls)
+    const int R = d->desc.rows, Cc = d->desc.cols;
+    std::vector<double> base((size_t)d->ntr * d->ntc, 1e300);
+    for (int r = 0; r < R; r++)
+      for (int c = 0; c < Cc; c++) {
+        double& b = base[(size_t)(r >> 5) * d->ntc + (c >> 5)];
+        b = std::min(b, host[(size_t)r * Cc + c]);
+      }
+    TRI_CUDA_TRY(cudaMemcpyAsync(d->zbase, base.data(), base.size() * 8, cudaMemcpyHostToDevice, d->stream));
+    TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+    k_bed_offsets<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, d->zbase, (float*)p, R, Cc, d->ntc);
+    TRI_CUDA_TRY(cudaGetLastError());
+    TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));  // 'base' leaves scope
   } else {
     TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
     k_from_f64<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, (float*)p, n);
@@ -539,6 +590,13 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   }
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
   if (field != TRI_FIELD_MAXH && field != TRI_FIELD_NMAN2) d->dt_valid = false;
+  if (field == TRI_FIELD_H) {  // a new state restarts the volume accounts
+    memset(d->mirror->acc_step, 0, sizeof(d->mirror->acc_step));
+    memset(d->mirror->acc_sum, 0, sizeof(d->mirror->acc_sum));
+    memset(d->mirror->acc_comp, 0, sizeof(d->mirror->acc_comp));
+    int rc2 = push_clock(d);
+    if (rc2 != TRI_OK) return rc2;
+  }
   return TRI_OK;
 }
 
@@ -550,6 +608,11 @@ int tri_domain_download(tri_domain* d, int32_t field, double* host, int64_t n) {
   if (rc != TRI_OK) return rc;
   if (d->prec == TRI_FP64) {
     TRI_CUDA_TRY(cudaMemcpyAsync(host, p, n * 8, cudaMemcpyDeviceToHost, d->stream));
+  } else if (field == TRI_FIELD_DEM) {
+    k_bed_levels<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const float*)p, d->zbase, d->stage,
+                                                                     d->desc.rows, d->desc.cols, d->ntc);
+    TRI_CUDA_TRY(cudaGetLastError());
+    TRI_CUDA_TRY(cudaMemcpyAsync(host, d->stage, n * 8, cudaMemcpyDeviceToHost, d->stream));
   } else {
     k_to_f64<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const float*)p, d->stage, n);
     TRI_CUDA_TRY(cudaGetLastError());
@@ -948,6 +1011,41 @@ int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile)
   d->rb = rows_per_tile;
   size_flux_grid(d);
   drop_graph(d);
+  return TRI_OK;
+}
+
+int tri_domain_mass_balance(tri_domain* d, double* out) {
+  TRI_CHECK_ARG(d && out, "null argument");
+  int rc = pull_clock(d);
+  if (rc != TRI_OK) return rc;
+  double vol = 0;
+  rc = tri_domain_volume(d, &vol);
+  if (rc != TRI_OK) return rc;
+  const double a = d->desc.cell_size * d->desc.cell_size;
+  out[0] = vol;
+  for (int k = 0; k < kAccTerms; k++) out[1 + k] = d->mirror->acc_sum[k] * a;
+  return TRI_OK;
+}
+
+int tri_domain_track_arrival(tri_domain* d, double depth) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (!d->arrival) TRI_CUDA_TRY(cudaMalloc((void**)&d->arrival, d->ncells * sizeof(float)));
+  std::vector<float> inf((size_t)d->ncells, 3.402823466e38f);
+  TRI_CUDA_TRY(cudaMemcpy(d->arrival, inf.data(), d->ncells * sizeof(float), cudaMemcpyHostToDevice));
+  d->arrival_depth = (float)depth;
+  drop_graph(d);
+  return TRI_OK;
+}
+
+int tri_domain_download_arrival(tri_domain* d, double* host, int64_t n) {
+  TRI_CHECK_ARG(d && host, "null argument");
+  TRI_CHECK_ARG(d->arrival, "arrival tracking is not enabled");
+  TRI_CHECK_ARG(n == d->ncells, "size %lld != rows*cols", (long long)n);
+  std::vector<float> tmp((size_t)n);
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  TRI_CUDA_TRY(cudaMemcpy(tmp.data(), d->arrival, n * sizeof(float), cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < n; i++) host[i] = tmp[i] >= 3.0e38f ? -1.0 : (double)tmp[i];
   return TRI_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <stdio.h>
 
 #include <string>
+#include <vector>
 
 #include "triton_b200.h"
 
@@ -28,5 +29,12 @@ int set_error(int code, const char* fmt, ...);
   } while (0)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Conflict-free waves: item k goes one wave after the latest earlier item
+// that touches one of its cells, so items sharing a cell keep their index
+// order and all others run in parallel.  'order' lists items wave by wave,
+// wave w is order[wave_start[w] .. wave_start[w+1]).
+void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<int32_t>& order,
+                 std::vector<int32_t>& wave_start);
 
 }  // namespace tri

@@ -5,6 +5,8 @@
 // domain path (tri_domain.cu) is the fast path.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "tri_face.cuh"
 #include "tri_internal.h"
 
@@ -270,14 +272,15 @@ __global__ void kr_wet_dry(int size, int nrows, int ncols, const double* __restr
   if (hij > maxh[id]) maxh[id] = hij;
 }
 
-__global__ void kr_extbc(int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy,
-                         const double* __restrict__ dem, const double* __restrict__ n,
+__global__ void kr_extbc(const int32_t* __restrict__ order, int count, int nrows, int ncols, double dt, double* h,
+                         double* qx, double* qy, const double* __restrict__ dem, const double* __restrict__ n,
                          const int32_t* __restrict__ rel, const int32_t* __restrict__ types,
                          const int32_t* __restrict__ start, const int32_t* __restrict__ nvars,
                          const double* __restrict__ v1, const double* __restrict__ v2, double simtime, int rank,
                          int nproc) {
-  const int id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= size) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int id = order[k];
   const int ii = rel[id], bt = types[id], s0 = start[id];
   const int ix = ii / ncols, iy = ii % ncols;
   const bool top = ix == 1, btm = ix == nrows - 2, lt = iy == 1, rt = iy == ncols - 2;
@@ -448,9 +451,39 @@ int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double d
                                         const int32_t* nrows_vars, const double* extbcvar1, const double* extbcvar2,
                                         double simtime, int rank, int total_process, void* stream) {
   if (size <= 0) return TRI_OK;
-  kr_extbc<<<nblocks(size), kThreads, 0, as_stream(stream)>>>(size, nrows, ncols, dt, h, qx, qy, dem, n,
-                                                             relative_index, extbctype, start_index, nrows_vars,
-                                                             extbcvar1, extbcvar2, simtime, rank, total_process);
+  TRI_CHECK_ARG(relative_index && extbctype && start_index && nrows_vars, "null device pointer");
+  // The cell list decides the application order: cells that touch the same
+  // cell run in index order (the reference's serial semantics), the rest in
+  // parallel.  The list is small (boundary cells); its waves are cached per
+  // list contents.
+  cudaStream_t s = as_stream(stream);
+  static thread_local std::vector<int32_t> last_cells, order, waves;
+  static thread_local int32_t* d_order = nullptr;
+  static thread_local size_t d_order_cap = 0;
+  std::vector<int32_t> cells((size_t)size);
+  TRI_CUDA_TRY(cudaMemcpyAsync(cells.data(), relative_index, size * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TRI_CUDA_TRY(cudaStreamSynchronize(s));
+  if (cells != last_cells) {
+    std::vector<std::vector<int64_t>> touch((size_t)size);
+    for (int i = 0; i < size; i++) {
+      const int64_t ii = cells[i];
+      touch[i] = {ii, ii - 1, ii + 1, ii - ncols, ii + ncols};
+    }
+    build_waves(touch, order, waves);
+    if (d_order_cap < order.size()) {
+      if (d_order) cudaFree(d_order);
+      TRI_CUDA_TRY(cudaMalloc((void**)&d_order, order.size() * sizeof(int32_t)));
+      d_order_cap = order.size();
+    }
+    TRI_CUDA_TRY(cudaMemcpy(d_order, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    last_cells = cells;
+  }
+  for (size_t w = 0; w + 1 < waves.size(); w++) {
+    const int off = waves[w], cnt = waves[w + 1] - off;
+    kr_extbc<<<nblocks(cnt), kThreads, 0, s>>>(d_order + off, cnt, nrows, ncols, dt, h, qx, qy, dem, n,
+                                                relative_index, extbctype, start_index, nrows_vars, extbcvar1,
+                                                extbcvar2, simtime, rank, total_process);
+  }
   return launched();
 }
 

@@ -21,6 +21,11 @@
 
 namespace tri {
 
+// Volume accounting terms of the FP32 form: inflow through boundary faces,
+// point sources, runoff, external-boundary depth resets, negative-depth clipping.
+constexpr int kAccTerms = 5;
+enum { kAccBoundary = 0, kAccSources = 1, kAccRunoff = 2, kAccExtbc = 3, kAccClip = 4 };
+
 // Device-resident loop state.  Host mirror: tri_clock plus the bookkeeping
 // fields below.
 struct DevClock {
@@ -39,6 +44,12 @@ struct DevClock {
   unsigned long long dt_key[2];
   const double* roff_t;
   const double* hyg_t;
+  // FP32 form: FP64 volume accounting in depth units (multiply by dx^2).
+  // acc_step collects the running step (atomics), the wet-dry kernel folds it
+  // into the Kahan-compensated totals acc_sum/acc_comp.
+  double acc_step[kAccTerms];
+  double acc_sum[kAccTerms];
+  double acc_comp[kAccTerms];
 };
 
 template <typename T>
@@ -47,6 +58,44 @@ struct StateBufs {
   T* qx[2];
   T* qy[2];
 };
+
+// The bed.  FP64 form: the DEM itself.  FP32 form: per 32x32 tile an FP64
+// base level and per cell an FP32 offset from it; kernels work with bed
+// levels relative to a nearby base ('ref'), so the differences that drive the
+// flux (bed steps, water level against a neighbour's bed) keep FP32 accuracy
+// on terrain hundreds of metres high.
+template <typename T>
+struct BedMap;
+template <>
+struct BedMap<double> {
+  const double* z;
+  const double* base;  // unused
+  int ntc;
+  __device__ __forceinline__ double ref_of(int, int) const { return 0.0; }
+  __device__ __forceinline__ double local(size_t id, int, int, double) const { return z[id]; }
+  __device__ __forceinline__ double absolute(size_t id, int, int) const { return z[id]; }
+};
+template <>
+struct BedMap<float> {
+  const float* z;      // offset from the tile base
+  const double* base;  // FP64 base level of each 32x32 tile
+  int ntc;             // tiles per row
+  __device__ __forceinline__ double ref_of(int r, int c) const { return base[(r >> 5) * ntc + (c >> 5)]; }
+  __device__ __forceinline__ float local(size_t id, int r, int c, double ref) const {
+    const double b = base[(r >> 5) * ntc + (c >> 5)];
+    return b == ref ? z[id] : z[id] + (float)(b - ref);
+  }
+  __device__ __forceinline__ double absolute(size_t id, int r, int c) const {
+    return base[(r >> 5) * ntc + (c >> 5)] + (double)z[id];
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 // ---------------------------------------------------------------------------
 // k_clock: the per-step scalar work of the reference host loop.
@@ -192,7 +241,7 @@ constexpr int kStripCols = 30;  // interior columns per warp strip
 
 template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
-                                                     const T* __restrict__ z, const T* __restrict__ n2,
+                                                     const BedMap<T> bed, const T* __restrict__ n2,
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
                                                      int rows, int cols, int rb, T dx, T rdx, T hextra) {
   if (!clk->active) return;
@@ -231,6 +280,10 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
     const bool upd = mid && c >= 1 && c <= cols - 2;
     const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this lane
     const bool owner = incol && (mid || gcol);
+    constexpr bool kAcct = sizeof(T) == 4;  // FP32 form keeps the FP64 volume accounts
+    double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
+    // bed levels relative to the base of the tile's first cell
+    const double zref = bed.ref_of(r0, min(sx * kStripCols + 1, cols - 1));
 
     auto copy_ghost = [&](int r) {
       const size_t id = (size_t)r * cols + c;
@@ -247,7 +300,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
         lh = hi[id];
         lqx = qxi[id];
         lqy = qyi[id];
-        lz = z[id];
+        lz = bed.local(id, r, c, zref);
       }
     };
     fetch(r0 - 1);
@@ -272,7 +325,18 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
         const size_t id = (size_t)(r - 1) * cols + c;
         T hn, qn, vn;
         update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn);
+        if (kAcct) {
+          // inflow through faces shared with ghost cells (depth units), and
+          // the depth the update clipped back to zero
+          if (c == 1) acc_b -= (double)pp.w0;
+          if (c == cols - 2) acc_b -= (double)pp.e0;
+          if (r - 1 == 1) acc_b -= (double)pp.n0;
+          if (r - 1 == rows - 2) acc_b -= (double)Y.b0;
+          const T raw = prev.h - (pp.e0 + pp.n0) - (pp.w0 + Y.b0);
+          if (raw < T(0)) acc_c -= (double)raw;
+        }
         if (nroff > 0) {  // update_runoff (kernels.h:128-149)
+          const T h0 = hn;
           const T net = rates[(size_t)zone[id] * roff_rows + roff_row];
           hn += net * dt;
           if (hn < hextra) {
@@ -280,6 +344,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
             qn = T(0);
             vn = T(0);
           }
+          if (kAcct) acc_r += (double)hn - (double)h0;
         }
         ho[id] = hn;
         qxo[id] = qn;
@@ -314,6 +379,16 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
       if (gcol) copy_ghost(r);
       prev = cur;
     }
+    if (kAcct) {
+      acc_b = warp_sum<T>(acc_b);
+      acc_r = warp_sum<T>(acc_r);
+      acc_c = warp_sum<T>(acc_c);
+      if (lane == 0) {
+        if (acc_b != 0.0) atomicAdd(&clk->acc_step[kAccBoundary], acc_b);
+        if (acc_r != 0.0) atomicAdd(&clk->acc_step[kAccRunoff], acc_r);
+        if (acc_c != 0.0) atomicAdd(&clk->acc_step[kAccClip], acc_c);
+      }
+    }
   }
 }
 
@@ -323,7 +398,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
 // same cell are in different waves, launched in the reference's index order.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_sources(const DevClock* __restrict__ clk, StateBufs<T> sb, const int32_t* __restrict__ order,
+__global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int32_t* __restrict__ order,
                           int count, int nsrc, const int32_t* __restrict__ cells, const double* __restrict__ hyg_t,
                           const T* __restrict__ hyg_v, T dx) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -349,6 +424,7 @@ __global__ void k_sources(const DevClock* __restrict__ clk, StateBufs<T> sb, con
   const T hs = (flow * dt) / (dx * dx);
   hij += hs;
   h[sid] = hij;
+  if (sizeof(T) == 4) atomicAdd(&clk->acc_step[kAccSources], (double)hs);
 }
 
 template <typename T>
@@ -384,7 +460,7 @@ __global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int
 }
 
 template <typename T>
-__global__ void k_extbc(const DevClock* __restrict__ clk, StateBufs<T> sb, const T* __restrict__ z,
+__global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMap<T> bed,
                         const T* __restrict__ n2, const int32_t* __restrict__ order, int count,
                         const int32_t* __restrict__ cells, const int32_t* __restrict__ types,
                         const int32_t* __restrict__ start, const int32_t* __restrict__ nrowsv,
@@ -485,7 +561,12 @@ __global__ void k_extbc(const DevClock* __restrict__ clk, StateBufs<T> sb, const
       const T td2 = var1[hi + s0] - var1[lo + s0];
       aux = var2[lo + s0] + (((var2[hi + s0] - var2[lo + s0]) * td) / td2);
     }
-    hij = dev_fmax(aux - z[ii], T(0));
+    if (sizeof(T) == 8) {
+      hij = dev_fmax(aux - (T)bed.absolute(ii, ix, iy), T(0));
+    } else {  // FP32 form: level minus bed in FP64, then rounded
+      hij = (T)fmax((double)aux - bed.absolute(ii, ix, iy), 0.0);
+      atomicAdd(&clk->acc_step[kAccExtbc], (double)hij - (double)h[ii]);
+    }
   } else {
     const T aux = var1[s0];
     T vel = T(0);
@@ -512,46 +593,111 @@ __global__ void k_extbc(const DevClock* __restrict__ clk, StateBufs<T> sb, const
 // of every cell (ghosts included, as compute_dt_and_sqrt runs over rows*cols)
 // reduced warp -> block -> one atomicMin on the ordered key of the slot the
 // next k_clock reads.  With WETDRY=false it is the initial dt pass.
+// Each thread walks one column down a band of rows, keeping h and the bed of
+// the rows above and below in registers and loading the next row one
+// iteration ahead; east/west neighbours come by shuffle (lanes 0 and 31 load
+// theirs).  Every value is read once, with several loads in flight.
 // ---------------------------------------------------------------------------
+constexpr int kWetCols = 128;
+
 template <typename T, bool WETDRY>
-__global__ void __launch_bounds__(256) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
-                                                   const T* __restrict__ z, T* __restrict__ maxh, int rows,
-                                                   int cols, T dx, T cn, T hextra) {
+__global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                        const BedMap<T> bed, T* __restrict__ maxh, int rows,
+                                                        int cols, int band, double dx, double cn, T hextra,
+                                                        float* __restrict__ arrival, float arrival_depth) {
   if (WETDRY && !clk->active) return;
+  if (sizeof(T) == 4 && WETDRY && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    // fold this step's volume terms into the Kahan-compensated totals
+    for (int k = 0; k < kAccTerms; k++) {
+      const double y = clk->acc_step[k] - clk->acc_comp[k];
+      const double t = clk->acc_sum[k] + y;
+      clk->acc_comp[k] = (t - clk->acc_sum[k]) - y;
+      clk->acc_sum[k] = t;
+      clk->acc_step[k] = 0.0;
+    }
+  }
   const int buf = WETDRY ? clk->dst : clk->cur;
   const int slot = WETDRY ? clk->wr : clk->rd;
   const T* __restrict__ h = sb.h[buf];
   T* __restrict__ qx = sb.qx[buf];
   T* __restrict__ qy = sb.qy[buf];
   const T E12 = eps12<T>();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kWetCols + threadIdx.x;
+  const int ra = blockIdx.y * band;
+  const int rz = min(ra + band - 1, rows - 1);
+  const bool incol = c < cols;
+  const bool intcol = c >= 1 && c <= cols - 2;
+  const double zref = bed.ref_of(ra, min(blockIdx.x * kWetCols, cols - 1));
+  const float simtime_now = WETDRY ? (float)clk->simtime : 0.0f;
+
+  T hm = T(0), zm = T(0), h0 = T(0), z0 = T(0), hp = T(0), zp = T(0);
+  T qx0 = T(0), qy0 = T(0), mh0 = T(0), qxp = T(0), qyp = T(0), mhp = T(0);
+  auto load_row = [&](int r, T& hv, T& zv, T& qxv, T& qyv, T& mhv) {
+    if (incol && r >= 0 && r < rows) {
+      const size_t id = (size_t)r * cols + c;
+      hv = h[id];
+      zv = bed.local(id, r, c, zref);
+      qxv = qx[id];
+      qyv = qy[id];
+      if (WETDRY && intcol && r >= 1 && r <= rows - 2) mhv = maxh[id];
+    }
+  };
+  {
+    T a, b, e;
+    if (ra >= 1) load_row(ra - 1, hm, zm, a, b, e);
+  }
+  load_row(ra, h0, z0, qx0, qy0, mh0);
   unsigned long long key = kDtKeyInf;
-  if (r < rows && c < cols) {
+  for (int r = ra; r <= rz; ++r) {
+    if (r + 1 <= rows - 1) load_row(r + 1, hp, zp, qxp, qyp, mhp);
+    // east / west neighbours of row r
+    T he = __shfl_down_sync(0xffffffffu, h0, 1), ze = __shfl_down_sync(0xffffffffu, z0, 1);
+    T hw = __shfl_up_sync(0xffffffffu, h0, 1), zw = __shfl_up_sync(0xffffffffu, z0, 1);
     const size_t id = (size_t)r * cols + c;
-    const T hij = h[id];
-    T qxv = qx[id], qyv = qy[id];
-    if (WETDRY && r >= 1 && r <= rows - 2 && c >= 1 && c <= cols - 2) {
-      const T zij = z[id];
+    const bool interior = WETDRY && intcol && r >= 1 && r <= rows - 2;
+    if (interior) {
+      if (lane == 31) {
+        he = h[id + 1];
+        ze = bed.local(id + 1, r, c + 1, zref);
+      }
+      if (lane == 0) {
+        hw = h[id - 1];
+        zw = bed.local(id - 1, r, c - 1, zref);
+      }
+    }
+    T qxv = qx0, qyv = qy0;
+    const T hij = h0;
+    if (interior) {
+      const T zij = z0;
       if (hij > hextra) {
-        const size_t e = id + 1, w = id - 1, n = id - cols, s = id + cols;
-        if ((hij + zij < z[e] && h[e] < E12) || (hij + zij < z[w] && h[w] < E12)) {
+        if ((hij + zij < ze && he < E12) || (hij + zij < zw && hw < E12)) {
           qxv = T(0);
           qx[id] = T(0);
         }
-        if ((hij + zij < z[n] && h[n] < E12) || (hij + zij < z[s] && h[s] < E12)) {
+        if ((hij + zij < zm && hm < E12) || (hij + zij < zp && hp < E12)) {
           qyv = T(0);
           qy[id] = T(0);
         }
       }
-      if (hij > maxh[id]) maxh[id] = hij;
+      if (hij > mh0) maxh[id] = hij;
+      if (arrival != nullptr && hij > arrival_depth && !(arrival[id] < 3.0e38f)) arrival[id] = simtime_now;
     }
-    if (hij > hextra) {
-      const T sq = dev_fmax(dev_sqrt(hij), T(0));
-      const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
-      const T dtc = cn * dx / (maxu + T(kSqrtG) * sq);
-      key = dt_key(dtc);
+    if (incol && hij > hextra) {  // CFL dt in FP64 in both forms
+      const double hd = (double)hij;
+      const double sq = fmax(sqrt(hd), 0.0);
+      const double maxu = fmax(fabs((double)qxv), fabs((double)qyv)) / hd;
+      const double dtc = cn * dx / (maxu + kSqrtG * sq);
+      const unsigned long long k = dt_key(dtc);
+      key = k < key ? k : key;
     }
+    hm = h0;
+    zm = z0;
+    h0 = hp;
+    z0 = zp;
+    qx0 = qxp;
+    qy0 = qyp;
+    mh0 = mhp;
   }
   // warp -> block -> device minimum
 #pragma unroll
@@ -559,20 +705,14 @@ __global__ void __launch_bounds__(256) k_wetdry_dt(DevClock* __restrict__ clk, S
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
     key = other < key ? other : key;
   }
-  __shared__ unsigned long long s_min[32];
-  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
-  const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  __shared__ unsigned long long s_min[kWetCols / 32];
+  const int warp = threadIdx.x >> 5;
   if (lane == 0) s_min[warp] = key;
   __syncthreads();
-  if (warp == 0) {
-    key = lane < nwarps ? s_min[lane] : kDtKeyInf;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
-      key = other < key ? other : key;
-    }
-    if (lane == 0 && key < kDtKeyInf) atomicMin(&clk->dt_key[slot], key);
+  if (threadIdx.x == 0) {
+    key = s_min[0];
+    for (int w = 1; w < kWetCols / 32; w++) key = s_min[w] < key ? s_min[w] : key;
+    if (key < kDtKeyInf) atomicMin(&clk->dt_key[slot], key);
   }
 }
 

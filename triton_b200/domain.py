@@ -149,6 +149,20 @@ class Domain:
         check(lib().tri_domain_volume(self._h, C.byref(v)))
         return v.value
 
+    def mass_balance(self):
+        """(volume, inflow_boundary, sources, runoff, extbc, clipping) in m^3."""
+        out = np.zeros(6)
+        check(lib().tri_domain_mass_balance(self._h, out.ctypes.data_as(_abi._dp)))
+        return dict(zip(("volume", "boundary", "sources", "runoff", "extbc", "clipping"), out.tolist()))
+
+    def track_arrival(self, depth=0.1):
+        check(lib().tri_domain_track_arrival(self._h, float(depth)))
+
+    def arrival(self):
+        a = np.empty(self.n)
+        check(lib().tri_domain_download_arrival(self._h, a.ctypes.data_as(_abi._dp), self.n))
+        return a.reshape(self.rows, self.cols)
+
     def synchronize(self):
         check(lib().tri_domain_synchronize(self._h))
 

@@ -228,29 +228,21 @@ def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, r
     z = _walls(dem)
     n2 = _copy_ghosts(_pad(mann)) ** 2
     zero = np.zeros_like(z)
-    # sources along the valley in the northern half
+    pi = print_interval or duration
+    sc = Scenario("watershed", dx, z, zero.copy(), zero.copy(), zero.copy(), n2, courant=0.5, hextra=0.001,
+                  sim_duration=duration, print_interval=pi, meta=dict(n=n, seed=seed, mann=mann))
+    # inflows along the valley in the northern half: 0 -> peak at 2 h -> 0 at 4 h
     src_rows = np.linspace(n * 0.1, n * 0.45, nsrc).astype(int)
     src_cols = (n / 2 + 0.15 * n * np.sin(2 * np.pi * src_rows / (0.6 * n))).astype(int)
-    cells = ((src_rows + 1) * (n + 2) + src_cols + 1).astype(np.int32)
-    times_h = np.array([0.0, 2.0, 4.0, 1000.0])
     flows = np.zeros((4, nsrc))
     flows[1, :] = peak_flow
-    sources = dict(cells=cells, times=times_h * 3600.0, flows=flows.reshape(-1), times_h=times_h,
-                   flows_rows=flows)
-    # uniform rain: one zone, rows (h, mm/h): (0, rain), (rain_hours, 0), (duration_h, 0)
-    rt_h = np.array([0.0, rain_hours, max(duration / 3600.0, rain_hours + 1.0)])
-    rr_mm = np.array([rain_mm_h, 0.0, 0.0])
-    runoff = dict(zone=np.zeros((n + 2, n + 2), dtype=np.int32), times=rt_h * 3600.0,
-                  rates=rr_mm / 3600.0 * 0.001, nzones=1, times_h=rt_h, rates_mm_h=rr_mm[:, None])
-    # open outflow along the southern edge (last interior row), type 0
-    bc_cells = ((n) * (n + 2) + np.arange(1, n + 1)).astype(np.int32)
-    extbc = dict(cells=bc_cells, types=np.zeros(n, np.int32), start=np.zeros(n, np.int32),
-                 nrows=np.ones(n, np.int32), var1=np.zeros(1), var2=np.zeros(1),
-                 segments=[(0, 0.0, dx * 0.5, n * dx - dx * 0.5, dx * 0.5, None)])
-    pi = print_interval or duration
-    return Scenario("watershed", dx, z, zero.copy(), zero.copy(), zero.copy(), n2, courant=0.5, hextra=0.001,
-                    sim_duration=duration, print_interval=pi, runoff=runoff, sources=sources, extbc=extbc,
-                    meta=dict(n=n, seed=seed))
+    sources_table(sc, list(zip(src_rows.tolist(), src_cols.tolist())), [0.0, 2.0, 4.0, 1000.0], flows)
+    # uniform rain on one zone: (0 h, rain), (rain_hours, 0), (end, 0)
+    end_h = max(duration / 3600.0, rain_hours + 1.0)
+    runoff_table(sc, np.zeros((n, n), dtype=np.int32), [0.0, rain_hours, end_h], [[rain_mm_h], [0.0], [0.0]])
+    # open outflow (type 0) along the southern edge, the lowest one
+    extbc_segments(sc, [(0, (n - 1, 0), (n - 1, n - 1), None)])
+    return sc
 
 
 def extbc_segments(sc, segments):
