@@ -18,7 +18,8 @@
 #include <vector>
 
 #include "tri_internal.h"
-#include "tri_step_kernels.cuh"
+#include "tri_step_launch.h"
+#include "tri_types.cuh"
 
 namespace tri {
 
@@ -141,17 +142,6 @@ StateBufs<T> bufs(tri_domain* d) {
   return s;
 }
 
-constexpr int kWetBand = 16;  // rows per block of the wet-dry/dt kernel
-
-template <typename T>
-BedMap<T> bedmap(tri_domain* d) {
-  BedMap<T> b;
-  b.z = (const T*)d->z;
-  b.base = d->zbase;
-  b.ntc = d->ntc;
-  return b;
-}
-
 void free_dev(void*& p) {
   if (p) cudaFree(p);
   p = nullptr;
@@ -239,33 +229,50 @@ __global__ void k_volume_sum(const double* __restrict__ part, int n, double scal
   *out = acc * scale;
 }
 
-// Register-budget variants of the flux kernel: at least 3, 4 or 5 resident
-// 128-thread blocks per SM (fewer registers per thread, more warps to hide
-// FP64 latency).  The autotuner picks one per domain.
-constexpr int kFluxVariants = 3;
-constexpr int kFluxMinBlocks[kFluxVariants] = {3, 4, 5};
-
-template <typename T>
-void flux_occupancy(int variant, int* per_sm) {
-  switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 3>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 4>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 5>, 128, 0); break;
+StepArgs step_args(tri_domain* d) {
+  StepArgs a{};
+  a.clk = d->clk;
+  for (int i = 0; i < 2; i++) {
+    a.h[i] = d->h[i];
+    a.qx[i] = d->qx[i];
+    a.qy[i] = d->qy[i];
   }
-}
-
-template <typename T>
-void launch_flux(tri_domain* d, StateBufs<T> sb, T dx, T hx) {
-  const int rows = d->desc.rows, cols = d->desc.cols;
-  const T rdx = (T)(1.0 / d->desc.cell_size);
-#define TRI_FLUX_ARGS                                                                                          \
-  d->clk, sb, bedmap<T>(d), (const T*)d->n2, d->zone, (const T*)d->rates, rows, cols, d->rb, dx, rdx, hx
-  switch (d->flux_variant) {
-    case 0: k_flux_update<T, 3><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
-    case 1: k_flux_update<T, 4><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
-    default: k_flux_update<T, 5><<<d->flux_blocks, 128, 0, d->stream>>>(TRI_FLUX_ARGS); break;
-  }
-#undef TRI_FLUX_ARGS
+  a.z = d->z;
+  a.zbase = d->zbase;
+  a.ntc = d->ntc;
+  a.n2 = d->n2;
+  a.maxh = d->maxh;
+  a.zone = d->zone;
+  a.rates = d->rates;
+  a.rows = d->desc.rows;
+  a.cols = d->desc.cols;
+  a.rb = d->rb;
+  a.flux_blocks = d->flux_blocks;
+  a.flux_variant = d->flux_variant;
+  a.dx = d->desc.cell_size;
+  a.courant = d->desc.courant;
+  a.hextra = d->desc.hextra;
+  a.open_boundaries = d->desc.open_boundaries;
+  a.nsrc = d->nsrc;
+  a.src_cells = d->src_cells;
+  a.src_order = d->src_order;
+  a.hyg_t = d->hyg_t;
+  a.hyg_v = d->hyg_v;
+  a.src_waves = d->src_waves.data();
+  a.n_src_waves = d->src_waves.empty() ? 0 : (int)d->src_waves.size() - 1;
+  a.nbc = d->nbc;
+  a.bc_cells = d->bc_cells;
+  a.bc_types = d->bc_types;
+  a.bc_start = d->bc_start;
+  a.bc_nrows = d->bc_nrows;
+  a.bc_order = d->bc_order;
+  a.bc_v1 = d->bc_v1;
+  a.bc_v2 = d->bc_v2;
+  a.bc_waves = d->bc_waves.data();
+  a.n_bc_waves = d->bc_waves.empty() ? 0 : (int)d->bc_waves.size() - 1;
+  a.arrival = d->arrival;
+  a.arrival_depth = d->arrival_depth;
+  return a;
 }
 
 // Grid of the flux kernel for the domain's variant and tile height: one
@@ -299,12 +306,7 @@ void choose_shape(tri_domain* d) {
   size_flux_grid(d);
 }
 
-template <typename T>
-int launch_step(tri_domain* d) {
-  const int rows = d->desc.rows, cols = d->desc.cols;
-  const T dx = (T)d->desc.cell_size, hx = (T)d->desc.hextra, cn = (T)d->desc.courant;
-  StateBufs<T> sb = bufs<T>(d);
-  k_clock<<<1, 32, 0, d->stream>>>(d->clk);
+int launch_one_step(tri_domain* d) {
   cudaEvent_t* ev = nullptr;
   if (d->timing) {
     while (d->tev.size() < d->tev_used + 4) {
@@ -314,49 +316,14 @@ int launch_step(tri_domain* d) {
     }
     ev = &d->tev[d->tev_used];
     d->tev_used += 4;
-    cudaEventRecord(ev[0], d->stream);
   }
-  launch_flux<T>(d, sb, dx, hx);
-  if (ev) cudaEventRecord(ev[1], d->stream);
-  if (d->nsrc > 0) {
-    for (size_t w = 0; w + 1 < d->src_waves.size(); w++) {
-      const int off = d->src_waves[w], cnt = d->src_waves[w + 1] - off;
-      k_sources<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, d->src_order + off, cnt, d->nsrc,
-                                                             d->src_cells, d->hyg_t, (const T*)d->hyg_v, dx);
-    }
-  }
-  if (d->desc.open_boundaries) {
-    const int n = std::max(rows, cols);
-    k_open_bc<T><<<(n + 255) / 256, 256, 0, d->stream>>>(d->clk, sb, rows, cols);
-  }
-  if (d->nbc > 0) {
-    for (size_t w = 0; w + 1 < d->bc_waves.size(); w++) {
-      const int off = d->bc_waves[w], cnt = d->bc_waves[w + 1] - off;
-      k_extbc<T><<<(cnt + 127) / 128, 128, 0, d->stream>>>(d->clk, sb, bedmap<T>(d), (const T*)d->n2,
-                                                           d->bc_order + off, cnt, d->bc_cells, d->bc_types,
-                                                           d->bc_start, d->bc_nrows, (const T*)d->bc_v1,
-                                                           (const T*)d->bc_v2, rows, cols);
-    }
-  }
-  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
-  if (ev) cudaEventRecord(ev[2], d->stream);
-  k_wetdry_dt<T, true><<<g2, kWetCols, 0, d->stream>>>(d->clk, sb, bedmap<T>(d), (T*)d->maxh, rows, cols,
-                                                       kWetBand, d->desc.cell_size, d->desc.courant, hx,
-                                                       d->arrival, d->arrival_depth);
-  if (ev) cudaEventRecord(ev[3], d->stream);
-  TRI_CUDA_TRY(cudaGetLastError());
-  return TRI_OK;
+  const StepArgs a = step_args(d);
+  return d->prec == TRI_FP64 ? launch_step<double>(a, d->stream, ev) : launch_step<float>(a, d->stream, ev);
 }
 
-template <typename T>
-int launch_initial_dt(tri_domain* d) {
-  const int rows = d->desc.rows, cols = d->desc.cols;
-  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
-  k_wetdry_dt<T, false><<<g2, kWetCols, 0, d->stream>>>(d->clk, bufs<T>(d), bedmap<T>(d), (T*)d->maxh, rows,
-                                                        cols, kWetBand, d->desc.cell_size, d->desc.courant,
-                                                        (T)d->desc.hextra, nullptr, 0.0f);
-  TRI_CUDA_TRY(cudaGetLastError());
-  return TRI_OK;
+int launch_dt(tri_domain* d) {
+  const StepArgs a = step_args(d);
+  return d->prec == TRI_FP64 ? launch_initial_dt<double>(a, d->stream) : launch_initial_dt<float>(a, d->stream);
 }
 
 int launch_steps(tri_domain* d, int n) {
@@ -367,7 +334,7 @@ int launch_steps(tri_domain* d, int n) {
       TRI_CUDA_TRY(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
       int rc = TRI_OK;
       for (int i = 0; i < G && rc == TRI_OK; i++)
-        rc = d->prec == TRI_FP64 ? launch_step<double>(d) : launch_step<float>(d);
+        rc = launch_one_step(d);
       cudaError_t e = cudaStreamEndCapture(d->stream, &g);
       if (rc != TRI_OK) {
         if (g) cudaGraphDestroy(g);
@@ -385,7 +352,7 @@ int launch_steps(tri_domain* d, int n) {
     }
   }
   for (int i = 0; i < n; i++) {
-    int rc = d->prec == TRI_FP64 ? launch_step<double>(d) : launch_step<float>(d);
+    int rc = launch_one_step(d);
     if (rc != TRI_OK) return rc;
   }
   return TRI_OK;
@@ -570,14 +537,17 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   if (d->prec == TRI_FP64) {
     TRI_CUDA_TRY(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, d->stream));
   } else if (field == TRI_FIELD_DEM) {
-    // base level of each 32x32 tile = its lowest cell (below the 1e6 walls)
+    // base level of each 32x32 tile = its lowest interior cell (ghost cells
+    // hold walls or copies and must not pull the base away from the terrain)
     const int R = d->desc.rows, Cc = d->desc.cols;
     std::vector<double> base((size_t)d->ntr * d->ntc, 1e300);
-    for (int r = 0; r < R; r++)
-      for (int c = 0; c < Cc; c++) {
+    for (int r = 1; r < R - 1; r++)
+      for (int c = 1; c < Cc - 1; c++) {
         double& b = base[(size_t)(r >> 5) * d->ntc + (c >> 5)];
         b = std::min(b, host[(size_t)r * Cc + c]);
       }
+    for (double& b : base)
+      if (b == 1e300) b = 0.0;
     TRI_CUDA_TRY(cudaMemcpyAsync(d->zbase, base.data(), base.size() * 8, cudaMemcpyHostToDevice, d->stream));
     TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
     k_bed_offsets<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, d->zbase, (float*)p, R, Cc, d->ntc);
@@ -823,7 +793,7 @@ int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* p) {
   int rc = push_clock(d);
   if (rc != TRI_OK) return rc;
   if (need_dt) {
-    rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+    rc = launch_dt(d);
     if (rc != TRI_OK) return rc;
   }
   d->dt_valid = true;
@@ -859,7 +829,7 @@ int tri_domain_compute_dt(tri_domain* d, double* local_dt) {
   m->dt_key[m->rd] = kDtKeyInf;
   int rc = push_clock(d);
   if (rc != TRI_OK) return rc;
-  rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+  rc = launch_dt(d);
   if (rc != TRI_OK) return rc;
   rc = pull_clock(d);
   if (rc != TRI_OK) return rc;
@@ -957,7 +927,7 @@ int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out) {
       m->halt = 0;
       m->dt_key[m->rd] = kDtKeyInf;
       rc = push_clock(d);
-      if (rc == TRI_OK) rc = d->prec == TRI_FP64 ? launch_initial_dt<double>(d) : launch_initial_dt<float>(d);
+      if (rc == TRI_OK) rc = launch_dt(d);
       if (rc == TRI_OK) rc = launch_steps(d, 2);  // warm-up (also builds the graph)
       cudaEventRecord(e0, d->stream);
       if (rc == TRI_OK) rc = launch_steps(d, trial_steps);

@@ -1,0 +1,8 @@
+// tri_step_f32.cu -- the step kernels instantiated for float.
+#include "tri_step_launch.cuh"
+
+namespace tri {
+template int launch_step<float>(const StepArgs&, cudaStream_t, cudaEvent_t*);
+template int launch_initial_dt<float>(const StepArgs&, cudaStream_t);
+template void flux_occupancy<float>(int, int*);
+}  // namespace tri

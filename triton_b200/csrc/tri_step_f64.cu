@@ -1,0 +1,8 @@
+// tri_step_f64.cu -- the step kernels instantiated for double.
+#include "tri_step_launch.cuh"
+
+namespace tri {
+template int launch_step<double>(const StepArgs&, cudaStream_t, cudaEvent_t*);
+template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);
+template void flux_occupancy<double>(int, int*);
+}  // namespace tri

@@ -18,46 +18,10 @@
 
 #include "tri_common.cuh"
 #include "tri_face.cuh"
+#include "tri_step_launch.h"
+#include "tri_types.cuh"
 
 namespace tri {
-
-// Volume accounting terms of the FP32 form: inflow through boundary faces,
-// point sources, runoff, external-boundary depth resets, negative-depth clipping.
-constexpr int kAccTerms = 5;
-enum { kAccBoundary = 0, kAccSources = 1, kAccRunoff = 2, kAccExtbc = 3, kAccClip = 4 };
-
-// Device-resident loop state.  Host mirror: tri_clock plus the bookkeeping
-// fields below.
-struct DevClock {
-  double simtime, sim_duration, print_interval, print_observation, last_obs_time;
-  double init_dt, time_step, average_dt, global_dt;
-  double t_step;  // simtime at the start of the running step
-  double rdt;     // RN(1/global_dt)
-  int32_t print_id, it_count, it_print, time_series, time_increment_fixed;
-  int32_t runoff_row, src_idx_low, src_idx_high;
-  int32_t active, halt, events, steps;
-  int32_t cur, src, dst, rd, wr;  // ping-pong state buffers and dt slots
-  int32_t nroff, roff_rows, nsrc, hyg_rows;
-  int32_t status;  // nonzero: a device-side check failed (value = reason)
-  uint32_t tile_next;  // work counter of the flux kernel's dynamic tiles, reset every step
-  uint32_t pad0;
-  unsigned long long dt_key[2];
-  const double* roff_t;
-  const double* hyg_t;
-  // FP32 form: FP64 volume accounting in depth units (multiply by dx^2).
-  // acc_step collects the running step (atomics), the wet-dry kernel folds it
-  // into the Kahan-compensated totals acc_sum/acc_comp.
-  double acc_step[kAccTerms];
-  double acc_sum[kAccTerms];
-  double acc_comp[kAccTerms];
-};
-
-template <typename T>
-struct StateBufs {
-  T* h[2];
-  T* qx[2];
-  T* qy[2];
-};
 
 // The bed.  FP64 form: the DEM itself.  FP32 form: per 32x32 tile an FP64
 // base level and per cell an FP32 offset from it; kernels work with bed
@@ -100,7 +64,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ---------------------------------------------------------------------------
 // k_clock: the per-step scalar work of the reference host loop.
 // ---------------------------------------------------------------------------
-__global__ void k_clock(DevClock* __restrict__ c) {
+static __global__ void k_clock(DevClock* __restrict__ c) {
   if (threadIdx.x != 0) return;
   if (c->halt) {
     c->active = 0;
@@ -237,7 +201,6 @@ __device__ __forceinline__ T shfl_down1(T v) {
   return __shfl_down_sync(0xffffffffu, v, 1);
 }
 
-constexpr int kStripCols = 30;  // interior columns per warp strip
 
 template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
@@ -598,8 +561,6 @@ __global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMa
 // iteration ahead; east/west neighbours come by shuffle (lanes 0 and 31 load
 // theirs).  Every value is read once, with several loads in flight.
 // ---------------------------------------------------------------------------
-constexpr int kWetCols = 128;
-
 template <typename T, bool WETDRY>
 __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                         const BedMap<T> bed, T* __restrict__ maxh, int rows,

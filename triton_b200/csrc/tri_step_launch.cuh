@@ -1,0 +1,91 @@
+// tri_step_launch.cuh -- definitions of the launch functions declared in
+// tri_step_launch.h; included by the two instantiation units only.
+#pragma once
+
+#include <algorithm>
+
+#include "tri_internal.h"
+#include "tri_step_kernels.cuh"
+#include "tri_step_launch.h"
+
+namespace tri {
+
+template <typename T>
+BedMap<T> bed_of(const StepArgs& a) {
+  BedMap<T> b;
+  b.z = (const T*)a.z;
+  b.base = a.zbase;
+  b.ntc = a.ntc;
+  return b;
+}
+
+template <typename T>
+StateBufs<T> bufs_of(const StepArgs& a) {
+  StateBufs<T> s;
+  for (int i = 0; i < 2; i++) {
+    s.h[i] = (T*)a.h[i];
+    s.qx[i] = (T*)a.qx[i];
+    s.qy[i] = (T*)a.qy[i];
+  }
+  return s;
+}
+
+template <typename T>
+void flux_occupancy(int variant, int* per_sm) {
+  switch (variant) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 3>, 128, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 4>, 128, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 5>, 128, 0); break;
+  }
+}
+
+template <typename T>
+int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  const int rows = a.rows, cols = a.cols;
+  const T dx = (T)a.dx, hx = (T)a.hextra, rdx = (T)(1.0 / a.dx);
+  StateBufs<T> sb = bufs_of<T>(a);
+  const BedMap<T> bed = bed_of<T>(a);
+  k_clock<<<1, 32, 0, s>>>(a.clk);
+  if (ev) cudaEventRecord(ev[0], s);
+#define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx
+  switch (a.flux_variant) {
+    case 0: k_flux_update<T, 3><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    case 1: k_flux_update<T, 4><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    default: k_flux_update<T, 5><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+  }
+#undef TRI_FLUX_ARGS
+  if (ev) cudaEventRecord(ev[1], s);
+  for (int w = 0; a.nsrc > 0 && w < a.n_src_waves; w++) {
+    const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
+    k_sources<T><<<(cnt + 127) / 128, 128, 0, s>>>(a.clk, sb, a.src_order + off, cnt, a.nsrc, a.src_cells, a.hyg_t,
+                                                   (const T*)a.hyg_v, dx);
+  }
+  if (a.open_boundaries) {
+    const int n = std::max(rows, cols);
+    k_open_bc<T><<<(n + 255) / 256, 256, 0, s>>>(a.clk, sb, rows, cols);
+  }
+  for (int w = 0; a.nbc > 0 && w < a.n_bc_waves; w++) {
+    const int off = a.bc_waves[w], cnt = a.bc_waves[w + 1] - off;
+    k_extbc<T><<<(cnt + 127) / 128, 128, 0, s>>>(a.clk, sb, bed, (const T*)a.n2, a.bc_order + off, cnt, a.bc_cells,
+                                                 a.bc_types, a.bc_start, a.bc_nrows, (const T*)a.bc_v1,
+                                                 (const T*)a.bc_v2, rows, cols);
+  }
+  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
+  if (ev) cudaEventRecord(ev[2], s);
+  k_wetdry_dt<T, true><<<g2, kWetCols, 0, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, kWetBand, a.dx, a.courant, hx,
+                                               a.arrival, a.arrival_depth);
+  if (ev) cudaEventRecord(ev[3], s);
+  TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
+template <typename T>
+int launch_initial_dt(const StepArgs& a, cudaStream_t s) {
+  dim3 g2((a.cols + kWetCols - 1) / kWetCols, (a.rows + kWetBand - 1) / kWetBand);
+  k_wetdry_dt<T, false><<<g2, kWetCols, 0, s>>>(a.clk, bufs_of<T>(a), bed_of<T>(a), (T*)a.maxh, a.rows, a.cols,
+                                                kWetBand, a.dx, a.courant, (T)a.hextra, nullptr, 0.0f);
+  TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
+}  // namespace tri

@@ -1,0 +1,69 @@
+// tri_step_launch.h -- host side of the step kernels: what one domain's
+// step needs (device pointers and sizes) and the launch functions.  The
+// kernels are instantiated in two translation units: tri_step_f64.cu (IEEE,
+// no contraction: bit-exact with the reference) and tri_step_f32.cu (FP32
+// precision form, contraction and fast division/sqrt allowed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tri_types.cuh"
+
+namespace tri {
+
+constexpr int kStripCols = 30;   // interior columns per warp tile of the flux kernel
+constexpr int kFluxVariants = 3; // register budgets: >= 3, 4, 5 blocks of 128 threads per SM
+constexpr int kWetCols = 128;    // columns per block of the wet-dry/dt kernel
+constexpr int kWetBand = 16;     // rows per block of the wet-dry/dt kernel
+
+struct StepArgs {
+  DevClock* clk;
+  void* h[2];
+  void* qx[2];
+  void* qy[2];
+  void* z;             // FP64 form: DEM; FP32 form: offsets from the tile bases
+  const double* zbase; // FP32 form: FP64 base level per 32x32 tile
+  int ntc;             // tiles per row
+  void* n2;
+  void* maxh;
+  const int32_t* zone;
+  const void* rates;
+  int rows, cols;
+  int rb, flux_blocks, flux_variant;
+  double dx, courant, hextra;
+  int open_boundaries;
+  int nsrc;
+  const int32_t* src_cells;
+  const int32_t* src_order;
+  const double* hyg_t;
+  const void* hyg_v;
+  const int32_t* src_waves;  // host array, n_src_waves + 1 offsets
+  int n_src_waves;
+  int nbc;
+  const int32_t *bc_cells, *bc_types, *bc_start, *bc_nrows, *bc_order;
+  const void *bc_v1, *bc_v2;
+  const int32_t* bc_waves;  // host array, n_bc_waves + 1 offsets
+  int n_bc_waves;
+  float* arrival;
+  float arrival_depth;
+};
+
+// One time step (clock, flux/update, sources, open ghosts, boundary cells,
+// wet-dry/dt).  ev: optional 4 events around the flux and wet-dry launches.
+template <typename T>
+int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev);
+// CFL dt of the current state into the slot the next step reads.
+template <typename T>
+int launch_initial_dt(const StepArgs& a, cudaStream_t s);
+template <typename T>
+void flux_occupancy(int variant, int* per_sm);
+
+extern template int launch_step<double>(const StepArgs&, cudaStream_t, cudaEvent_t*);
+extern template int launch_step<float>(const StepArgs&, cudaStream_t, cudaEvent_t*);
+extern template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);
+extern template int launch_initial_dt<float>(const StepArgs&, cudaStream_t);
+extern template void flux_occupancy<double>(int, int*);
+extern template void flux_occupancy<float>(int, int*);
+
+}  // namespace tri
