@@ -101,7 +101,8 @@ typedef struct tri_clock {
   int32_t time_increment_fixed;
   int32_t runoff_row;  /* index_row_runoff (triton_init.h:1299-1310) */
   int32_t src_idx_low; /* idx_low of the hydrograph search (triton.h:79) */
-  int32_t reserved;
+  int32_t last_events; /* out: OR of TRI_EV_* raised by the last advance
+                          (domain or batch); ignored by set_clock */
 } tri_clock;
 
 typedef struct tri_progress {
@@ -202,6 +203,36 @@ int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile)
  * n pseudo-random (a, b) pairs from 'seed' over the magnitudes the step
  * produces; counts quotients that differ in any bit from IEEE a/b. */
 int tri_selftest_division(int64_t n, uint64_t seed, int64_t* mismatches);
+
+/* ---- batches of member domains ------------------------------------------ */
+/* Ensemble members advanced together on one GPU.  Replaces the reference's
+ * ensemble runs (src/Ensify.h:43-72), which give every member its own group
+ * of MPI ranks and processes.  Each batched step moves every member by one of
+ * its own time steps (own dt policy, own events); one launch per kernel type
+ * covers all members, the flux kernel taking tiles from a single queue over
+ * all members.  Members stay tri_domain objects: upload, download, forcing,
+ * observe and set_clock work on them between batch advances.  Members must
+ * share one precision and have open_boundaries = 0.  A member whose forcing
+ * changes after tri_batch_create needs a new batch. */
+typedef struct tri_batch tri_batch;
+typedef struct tri_batch_progress {
+  int32_t steps;               /* most steps any member took */
+  int32_t members_with_events; /* members that stopped on an event */
+  int32_t members_ended;       /* members with simtime >= sim_duration */
+  int32_t reserved;
+  int64_t cell_updates;        /* sum over members of steps x interior cells */
+} tri_batch_progress;
+/* stream: cudaStream_t for the batched launches, NULL = the batch makes one. */
+int tri_batch_create(int32_t nmembers, tri_domain* const* members, void* stream, tri_batch** out);
+int tri_batch_destroy(tri_batch* b);
+/* Advances every member until it raises an event (its clock then halts, as in
+ * tri_domain_advance) or until max_steps batched steps have run.  Members
+ * already at their end take no steps.  Blocks until done. */
+int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* out);
+/* Launch-shape autotuner of the batched flux kernel; members' states, maximum
+ * depths and clocks are restored afterwards. */
+int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out);
+int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile);
 
 /* ---- reference kernels (FP64, device pointers) -------------------------- */
 /* Each launches on 'stream' (cudaStream_t, NULL = default stream) and does not

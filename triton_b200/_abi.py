@@ -32,7 +32,7 @@ class Clock(C.Structure):
                 ("time_step", C.c_double), ("average_dt", C.c_double), ("global_dt", C.c_double),
                 ("print_id", C.c_int32), ("it_count", C.c_int32), ("it_print", C.c_int32),
                 ("time_series", C.c_int32), ("time_increment_fixed", C.c_int32), ("runoff_row", C.c_int32),
-                ("src_idx_low", C.c_int32), ("reserved", C.c_int32)]
+                ("src_idx_low", C.c_int32), ("last_events", C.c_int32)]
 
 
 class Progress(C.Structure):
@@ -42,6 +42,11 @@ class Progress(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("variant", C.c_int32), ("rows_per_tile", C.c_int32), ("candidates", C.c_int32),
                 ("flux_blocks", C.c_int32), ("ms_per_step", C.c_double)]
+
+
+class BatchProgress(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("members_with_events", C.c_int32), ("members_ended", C.c_int32),
+                ("reserved", C.c_int32), ("cell_updates", C.c_int64)]
 
 
 class TriError(RuntimeError):
@@ -78,6 +83,11 @@ _SIGS = {
     "tri_domain_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_domain_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
     "tri_domain_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "tri_batch_create": (C.c_int, [C.c_int32, C.POINTER(_vp), _vp, C.POINTER(_vp)]),
+    "tri_batch_destroy": (C.c_int, [_vp]),
+    "tri_batch_advance": (C.c_int, [_vp, C.c_int32, C.POINTER(BatchProgress)]),
+    "tri_batch_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
+    "tri_batch_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "tri_selftest_division": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     "tri_kernel_compute_dt_and_sqrt_f64": (C.c_int, [C.c_int, C.c_double, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                                      C.c_double, _vp]),

@@ -1,0 +1,455 @@
+// tri_batch.cu -- tri_batch_*: ensembles of member domains advanced together.
+//
+// The reference runs ensemble members as separate MPI rank groups (Ensify,
+// src/Ensify.h:43-72), one process group per member.  Here every member is a
+// tri_domain on one GPU and a batched step advances each member by one of its
+// own time steps with one launch per kernel type: a clock kernel over the
+// member table (per-member dt policy and events), one flux kernel whose warps
+// take tiles from a single queue over all members' tiles (uneven sizes pack
+// without idle SMs), the sparse forcing in conflict-free waves of (member,
+// item) pairs, and one wet-dry/dt kernel over all members' bands, each member
+// folding its own dt minimum.  Steps are launched as CUDA graphs of 8 batched
+// steps; the host checks after each graph how many members have halted.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "tri_domain_impl.h"
+#include "tri_internal.h"
+#include "tri_step_launch.h"
+
+using namespace tri;
+
+struct tri_batch {
+  int prec = TRI_FP64;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<tri_domain*> members;
+  void* d_mem = nullptr;
+  BatchCtl* d_ctl = nullptr;
+  BatchCtl* h_ctl = nullptr;  // pinned
+  int32_t* h_seen = nullptr;  // pinned, one per chunk slot
+  uint32_t ntiles = 0, nwet = 0;
+  int rb = 8, variant = 1, flux_blocks = 1;
+  int2* d_src_items = nullptr;
+  std::vector<int32_t> src_waves;
+  int2* d_bc_items = nullptr;
+  std::vector<int32_t> bc_waves;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  double tuned_ms = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+template <typename T>
+MemberDev<T> member_dev(tri_domain* d, int rb, uint32_t& tiles, uint32_t& wet) {
+  const StepArgs a = domain_step_args(d);
+  MemberDev<T> m{};
+  m.clk = d->clk;
+  for (int i = 0; i < 2; i++) {
+    m.sb.h[i] = (T*)a.h[i];
+    m.sb.qx[i] = (T*)a.qx[i];
+    m.sb.qy[i] = (T*)a.qy[i];
+  }
+  m.bed.z = (const T*)a.z;
+  m.bed.base = a.zbase;
+  m.bed.ntc = a.ntc;
+  m.n2 = (const T*)a.n2;
+  m.zone = a.zone;
+  m.rates = (const T*)a.rates;
+  m.maxh = (T*)a.maxh;
+  m.arrival = a.arrival;
+  m.arrival_depth = a.arrival_depth;
+  m.rows = a.rows;
+  m.cols = a.cols;
+  m.rb = rb;
+  m.dx = (T)a.dx;
+  m.rdx = (T)(1.0 / a.dx);
+  m.hextra = (T)a.hextra;
+  m.dxd = a.dx;
+  m.courant = a.courant;
+  const uint32_t strips = (uint32_t)((a.cols - 2 + kStripCols - 1) / kStripCols);
+  const uint32_t rowb = (uint32_t)((a.rows - 2 + rb - 1) / rb);
+  m.tile_begin = tiles;
+  tiles += strips * rowb;
+  m.tile_end = tiles;
+  m.wet_nbx = (uint32_t)((a.cols + kWetCols - 1) / kWetCols);
+  m.wet_begin = wet;
+  wet += m.wet_nbx * (uint32_t)((a.rows + kWetBand - 1) / kWetBand);
+  m.nsrc = a.nsrc;
+  m.src_cells = a.src_cells;
+  m.hyg_t = a.hyg_t;
+  m.hyg_v = (const T*)a.hyg_v;
+  m.bc_cells = a.bc_cells;
+  m.bc_types = a.bc_types;
+  m.bc_start = a.bc_start;
+  m.bc_nrows = a.bc_nrows;
+  m.bc_v1 = (const T*)a.bc_v1;
+  m.bc_v2 = (const T*)a.bc_v2;
+  return m;
+}
+
+void drop_graph(tri_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_steps = 0;
+}
+
+// Member table, tile and block counts, grid of the flux kernel.
+template <typename T>
+int build_table(tri_batch* b) {
+  std::vector<MemberDev<T>> tab;
+  uint32_t tiles = 0, wet = 0;
+  for (tri_domain* d : b->members) tab.push_back(member_dev<T>(d, b->rb, tiles, wet));
+  b->ntiles = tiles;
+  b->nwet = wet;
+  if (b->d_mem) cudaFree(b->d_mem);
+  b->d_mem = nullptr;
+  TRI_CUDA_TRY(cudaMalloc(&b->d_mem, tab.size() * sizeof(MemberDev<T>)));
+  TRI_CUDA_TRY(cudaMemcpy(b->d_mem, tab.data(), tab.size() * sizeof(MemberDev<T>), cudaMemcpyHostToDevice));
+  int sms = 148, dev = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  batch_flux_occupancy<T>(b->variant, &per_sm);
+  if (per_sm < 1) per_sm = 1;
+  b->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
+  drop_graph(b);
+  return TRI_OK;
+}
+
+int rebuild(tri_batch* b) { return b->prec == TRI_FP64 ? build_table<double>(b) : build_table<float>(b); }
+
+// (member, item) pairs of every member's conflict-free waves, wave by wave.
+int build_items(tri_batch* b) {
+  auto gather = [&](bool src, int2** dptr, std::vector<int32_t>& waves) -> int {
+    std::vector<std::vector<int2>> per;
+    for (size_t m = 0; m < b->members.size(); m++) {
+      tri_domain* d = b->members[m];
+      const std::vector<int32_t>& w = src ? d->src_waves : d->bc_waves;
+      const std::vector<int32_t>& o = src ? d->src_order_host : d->bc_order_host;
+      const int n = src ? d->nsrc : d->nbc;
+      if (n <= 0 || w.size() < 2) continue;
+      for (size_t k = 0; k + 1 < w.size(); k++) {
+        if (per.size() <= k) per.resize(k + 1);
+        for (int j = w[k]; j < w[k + 1]; j++) per[k].push_back(make_int2((int)m, o[j]));
+      }
+    }
+    std::vector<int2> flat;
+    waves.assign(1, 0);
+    for (auto& v : per) {
+      flat.insert(flat.end(), v.begin(), v.end());
+      waves.push_back((int32_t)flat.size());
+    }
+    if (*dptr) cudaFree(*dptr);
+    *dptr = nullptr;
+    if (!flat.empty()) {
+      TRI_CUDA_TRY(cudaMalloc((void**)dptr, flat.size() * sizeof(int2)));
+      TRI_CUDA_TRY(cudaMemcpy(*dptr, flat.data(), flat.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    }
+    return TRI_OK;
+  };
+  int rc = gather(true, &b->d_src_items, b->src_waves);
+  if (rc == TRI_OK) rc = gather(false, &b->d_bc_items, b->bc_waves);
+  return rc;
+}
+
+BatchArgs batch_args(tri_batch* b) {
+  BatchArgs a{};
+  a.mem = b->d_mem;
+  a.nm = (int)b->members.size();
+  a.ctl = b->d_ctl;
+  a.ntiles = b->ntiles;
+  a.nwet_blocks = b->nwet;
+  a.flux_blocks = b->flux_blocks;
+  a.flux_variant = b->variant;
+  a.src_items = b->d_src_items;
+  a.src_waves = b->src_waves.data();
+  a.n_src_waves = (int)b->src_waves.size() - 1;
+  a.bc_items = b->d_bc_items;
+  a.bc_waves = b->bc_waves.data();
+  a.n_bc_waves = (int)b->bc_waves.size() - 1;
+  return a;
+}
+
+int launch_batch(tri_batch* b, int n) {
+  const BatchArgs a = batch_args(b);
+  auto one = [&]() {
+    return b->prec == TRI_FP64 ? launch_batch_step<double>(a, b->stream) : launch_batch_step<float>(a, b->stream);
+  };
+  const int G = 8;
+  if (!b->graph) {
+    cudaGraph_t g = nullptr;
+    TRI_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = TRI_OK;
+    for (int i = 0; i < G && rc == TRI_OK; i++) rc = one();
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc != TRI_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_error(TRI_E_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_error(TRI_E_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+    b->graph_steps = G;
+  }
+  while (n >= b->graph_steps) {
+    TRI_CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    n -= b->graph_steps;
+  }
+  for (int i = 0; i < n; i++) {
+    int rc = one();
+    if (rc != TRI_OK) return rc;
+  }
+  return TRI_OK;
+}
+
+// Prepares every member's clock for a batched advance (members at or past
+// their end stay halted for the whole call); counts the members that step.
+int prepare_members(tri_batch* b, int* runnable) {
+  *runnable = 0;
+  for (tri_domain* d : b->members) {
+    DevClock* m = d->mirror;
+    const bool live = m->simtime < m->sim_duration;
+    m->halt = live ? 0 : 1;
+    m->events = 0;
+    m->steps = 0;
+    const bool need_dt = live && !d->dt_valid && !m->time_increment_fixed;
+    if (need_dt) m->dt_key[m->rd] = kDtKeyInf;
+    int rc = domain_push_clock(d);
+    if (rc != TRI_OK) return rc;
+    if (need_dt) {
+      rc = domain_launch_dt(d);
+      if (rc != TRI_OK) return rc;
+      d->dt_valid = true;
+    }
+    if (live) (*runnable)++;
+  }
+  for (tri_domain* d : b->members) TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tri_batch_create(int32_t nmembers, tri_domain* const* members, void* stream, tri_batch** out) {
+  TRI_CHECK_ARG(out && members && nmembers >= 1, "need at least one member");
+  *out = nullptr;
+  tri_batch* b = new tri_batch();
+  b->prec = members[0] ? members[0]->prec : TRI_FP64;
+  for (int i = 0; i < nmembers; i++) {
+    tri_domain* d = members[i];
+    if (!d || d->prec != b->prec || d->desc.open_boundaries) {
+      delete b;
+      return set_error(TRI_E_INVALID,
+                       "batch member %d: members must exist, share one precision and use closed or "
+                       "external-boundary edges (open_boundaries=0)",
+                       i);
+    }
+    for (int j = 0; j < i; j++)
+      if (members[j] == d) {
+        delete b;
+        return set_error(TRI_E_INVALID, "batch member %d repeats member %d", i, j);
+      }
+    b->members.push_back(d);
+  }
+  int rc = TRI_OK;
+  auto fail = [&](int code) {
+    tri_batch_destroy(b);
+    return code;
+  };
+  if (stream) {
+    b->stream = as_stream(stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(set_error(TRI_E_CUDA, "cannot create a CUDA stream"));
+    b->own_stream = true;
+  }
+  if (cudaMalloc((void**)&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+      cudaMallocHost((void**)&b->h_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+      cudaMallocHost((void**)&b->h_seen, 2 * sizeof(int32_t)) != cudaSuccess)
+    return fail(set_error(TRI_E_CUDA, "batch control allocation failed"));
+  cudaEventCreateWithFlags(&b->ev[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&b->ev[1], cudaEventDisableTiming);
+  // the members' own streams must be idle before the batch uses their memory
+  for (tri_domain* d : b->members) cudaStreamSynchronize(d->stream);
+  if ((rc = rebuild(b)) != TRI_OK) return fail(rc);
+  if ((rc = build_items(b)) != TRI_OK) return fail(rc);
+  *out = b;
+  return TRI_OK;
+}
+
+int tri_batch_destroy(tri_batch* b) {
+  if (!b) return TRI_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  if (b->d_mem) cudaFree(b->d_mem);
+  if (b->d_ctl) cudaFree(b->d_ctl);
+  if (b->h_ctl) cudaFreeHost(b->h_ctl);
+  if (b->h_seen) cudaFreeHost(b->h_seen);
+  if (b->d_src_items) cudaFree(b->d_src_items);
+  if (b->d_bc_items) cudaFree(b->d_bc_items);
+  for (int i = 0; i < 2; i++)
+    if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return TRI_OK;
+}
+
+int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* p) {
+  TRI_CHECK_ARG(b && p, "null argument");
+  TRI_CHECK_ARG(max_steps >= 0, "max_steps must be >= 0");
+  memset(p, 0, sizeof(*p));
+  int runnable = 0;
+  int rc = prepare_members(b, &runnable);
+  if (rc != TRI_OK) return rc;
+  if (runnable > 0 && max_steps > 0) {
+    b->h_ctl->halted = 0;
+    b->h_ctl->tile_next = 0;
+    TRI_CUDA_TRY(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
+    // chunks of 8 batched steps, two in flight; stop once every runnable
+    // member has raised an event
+    int left = max_steps, k = 0;
+    bool done = false;
+    while (left > 0 && !done) {
+      const int n = std::min(8, left);
+      rc = launch_batch(b, n);
+      if (rc != TRI_OK) return rc;
+      TRI_CUDA_TRY(cudaMemcpyAsync(&b->h_seen[k & 1], &b->d_ctl->halted, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   b->stream));
+      TRI_CUDA_TRY(cudaEventRecord(b->ev[k & 1], b->stream));
+      left -= n;
+      if (k > 0) {
+        TRI_CUDA_TRY(cudaEventSynchronize(b->ev[(k - 1) & 1]));
+        if (b->h_seen[(k - 1) & 1] >= runnable) done = true;
+      }
+      k++;
+    }
+    TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  }
+  int64_t updates = 0;
+  for (tri_domain* d : b->members) {
+    TRI_CUDA_TRY(cudaMemcpy(d->mirror, d->clk, sizeof(DevClock), cudaMemcpyDeviceToHost));
+    const DevClock* m = d->mirror;
+    p->steps = std::max(p->steps, m->steps);
+    if (m->events) p->members_with_events++;
+    if (!(m->simtime < m->sim_duration)) p->members_ended++;
+    updates += (int64_t)m->steps * (int64_t)(d->desc.rows - 2) * (int64_t)(d->desc.cols - 2);
+  }
+  p->cell_updates = updates;
+  return TRI_OK;
+}
+
+int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile) {
+  TRI_CHECK_ARG(b, "null batch");
+  TRI_CHECK_ARG(variant >= 0 && variant < kFluxVariants, "variant %d outside [0,%d)", variant, kFluxVariants);
+  TRI_CHECK_ARG(rows_per_tile >= 1, "rows_per_tile must be >= 1");
+  TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  b->variant = variant;
+  b->rb = rows_per_tile;
+  return rebuild(b);
+}
+
+int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out) {
+  TRI_CHECK_ARG(b && out, "null argument");
+  TRI_CHECK_ARG(trial_steps >= 1, "trial_steps must be >= 1");
+  // snapshot every member: current state, max depth and clock
+  struct Snap {
+    void* buf = nullptr;
+    DevClock clk;
+    bool valid = false;
+  };
+  std::vector<Snap> snaps(b->members.size());
+  int rc = TRI_OK;
+  for (size_t i = 0; i < b->members.size() && rc == TRI_OK; i++) {
+    tri_domain* d = b->members[i];
+    const size_t fb = d->ncells * d->esize;
+    if (cudaMalloc(&snaps[i].buf, 4 * fb) != cudaSuccess) {
+      rc = set_error(TRI_E_NOMEM, "autotune snapshot allocation failed");
+      break;
+    }
+    const int cur = d->mirror->cur;
+    void* f[4] = {d->h[cur], d->qx[cur], d->qy[cur], d->maxh};
+    for (int k = 0; k < 4; k++) cudaMemcpy((char*)snaps[i].buf + k * fb, f[k], fb, cudaMemcpyDeviceToDevice);
+    snaps[i].clk = *d->mirror;
+    snaps[i].valid = d->dt_valid;
+  }
+  auto restore = [&]() -> int {
+    for (size_t i = 0; i < b->members.size(); i++) {
+      tri_domain* d = b->members[i];
+      const size_t fb = d->ncells * d->esize;
+      *d->mirror = snaps[i].clk;
+      d->dt_valid = snaps[i].valid;
+      const int cur = d->mirror->cur;
+      void* f[4] = {d->h[cur], d->qx[cur], d->qy[cur], d->maxh};
+      for (int k = 0; k < 4; k++)
+        TRI_CUDA_TRY(cudaMemcpy(f[k], (char*)snaps[i].buf + k * fb, fb, cudaMemcpyDeviceToDevice));
+      int r = domain_push_clock(d);
+      if (r != TRI_OK) return r;
+      TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+    }
+    return TRI_OK;
+  };
+  const int heights[3] = {4, 8, 16};
+  double best = 1e300;
+  int best_v = b->variant, best_rb = b->rb, ncand = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int v = 0; v < kFluxVariants && rc == TRI_OK; v++) {
+    for (int hi = 0; hi < 3 && rc == TRI_OK; hi++) {
+      b->variant = v;
+      b->rb = heights[hi];
+      rc = rebuild(b);
+      if (rc == TRI_OK) rc = restore();
+      for (tri_domain* d : b->members) {  // trials run without events
+        d->mirror->sim_duration = d->mirror->print_interval = d->mirror->print_observation = 1e300;
+        d->mirror->it_print = 0;
+        d->mirror->time_series = 0;
+      }
+      int runnable = 0;
+      if (rc == TRI_OK) rc = prepare_members(b, &runnable);
+      if (rc == TRI_OK) {
+        b->h_ctl->halted = 0;
+        cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream);
+        rc = launch_batch(b, 2);  // warm-up, also builds the graph
+      }
+      cudaEventRecord(e0, b->stream);
+      if (rc == TRI_OK) rc = launch_batch(b, trial_steps);
+      cudaEventRecord(e1, b->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess && rc == TRI_OK)
+        rc = set_error(TRI_E_CUDA, "batch autotune trial failed");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ncand++;
+      if (rc == TRI_OK && ms / trial_steps < best) {
+        best = ms / trial_steps;
+        best_v = v;
+        best_rb = heights[hi];
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->variant = best_v;
+  b->rb = best_rb;
+  int rc2 = rebuild(b);
+  if (rc2 == TRI_OK && snaps.size() && snaps.back().buf) rc2 = restore();
+  for (Snap& s : snaps)
+    if (s.buf) cudaFree(s.buf);
+  if (rc != TRI_OK) return rc;
+  if (rc2 != TRI_OK) return rc2;
+  b->tuned_ms = best;
+  out->variant = b->variant;
+  out->rows_per_tile = b->rb;
+  out->candidates = ncand;
+  out->flux_blocks = b->flux_blocks;
+  out->ms_per_step = best;
+  return TRI_OK;
+}
+
+}  // extern "C"

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "tri_internal.h"
+#include "tri_domain_impl.h"
 #include "tri_step_launch.h"
 #include "tri_types.cuh"
 
@@ -63,71 +64,6 @@ void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<i
 }  // namespace tri
 
 using namespace tri;
-
-struct tri_domain {
-  tri_grid_desc desc{};
-  int prec = TRI_FP64;
-  size_t esize = 8;
-  int64_t ncells = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  // state (ping-pong) and static fields; element type double or float
-  void* h[2] = {nullptr, nullptr};
-  void* qx[2] = {nullptr, nullptr};
-  void* qy[2] = {nullptr, nullptr};
-  void* z = nullptr;
-  void* n2 = nullptr;
-  void* maxh = nullptr;
-  double* stage = nullptr;  // FP64 staging field for FP32 uploads/downloads
-  double* zbase = nullptr;  // FP32 form: FP64 bed base level per 32x32 tile
-  int ntc = 0, ntr = 0;     // tiles per row / per column
-  float* arrival = nullptr; // optional first time h exceeds arrival_depth
-  float arrival_depth = 0.1f;
-  // runoff
-  int32_t nroff = 0, roff_rows = 0;
-  int32_t* zone = nullptr;
-  void* rates = nullptr;
-  double* roff_t = nullptr;
-  // sources
-  int32_t nsrc = 0, hyg_rows = 0;
-  int32_t* src_cells = nullptr;
-  int32_t* src_order = nullptr;
-  std::vector<int32_t> src_waves;
-  double* hyg_t = nullptr;
-  void* hyg_v = nullptr;
-  // external boundary cells
-  int32_t nbc = 0;
-  int32_t *bc_cells = nullptr, *bc_types = nullptr, *bc_start = nullptr, *bc_nrows = nullptr, *bc_order = nullptr;
-  std::vector<int32_t> bc_waves;
-  void *bc_v1 = nullptr, *bc_v2 = nullptr;
-  // observations
-  int32_t nobs = 0;
-  int32_t* obs_cells = nullptr;
-  double* obs_out = nullptr;
-  double* obs_host = nullptr;
-  // clock
-  DevClock* clk = nullptr;  // device
-  DevClock* mirror = nullptr;  // pinned host mirror
-  int32_t* halt_host = nullptr;  // pinned, one per chunk slot
-  bool dt_valid = false;
-  // volume reduction scratch
-  double* vol_part = nullptr;
-  double* vol_out = nullptr;
-  int vol_blocks = 0;
-  // launch shape of the flux kernel (tile height, register variant, grid)
-  int rb = 16, flux_blocks = 1, flux_variant = 0;
-  double tuned_ms = 0;
-  // graphs of 'graph_steps' steps
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  bool use_graphs = true;
-  // timing: CUDA event pairs around every flux and wet-dry launch, read once
-  // the timed region is over so the stream is never stalled
-  bool timing = false;
-  std::vector<cudaEvent_t> tev;
-  size_t tev_used = 0;
-  cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
-};
 
 namespace {
 
@@ -405,6 +341,13 @@ int pull_clock(tri_domain* d) {
 
 }  // namespace
 
+namespace tri {
+int domain_push_clock(tri_domain* d) { return push_clock(d); }
+int domain_pull_clock(tri_domain* d) { return pull_clock(d); }
+int domain_launch_dt(tri_domain* d) { return launch_dt(d); }
+StepArgs domain_step_args(tri_domain* d) { return step_args(d); }
+}  // namespace tri
+
 extern "C" {
 
 int tri_abi_version(void) { return TRI_ABI_VERSION; }
@@ -646,6 +589,7 @@ int tri_domain_set_sources(tri_domain* d, int32_t nsrc, const int32_t* cells, in
   }
   std::vector<int32_t> order;
   build_waves(touch, order, d->src_waves);
+  d->src_order_host = order;
   int rc;
   if ((rc = upload_raw(d, cells, nsrc * 4, (void**)&d->src_cells)) != TRI_OK) return rc;
   if ((rc = upload_raw(d, order.data(), order.size() * 4, (void**)&d->src_order)) != TRI_OK) return rc;
@@ -687,6 +631,7 @@ int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, co
   }
   std::vector<int32_t> order;
   build_waves(touch, order, d->bc_waves);
+  d->bc_order_host = order;
   int rc;
   if ((rc = upload_raw(d, cells, ncells * 4, (void**)&d->bc_cells)) != TRI_OK) return rc;
   if ((rc = upload_raw(d, types, ncells * 4, (void**)&d->bc_types)) != TRI_OK) return rc;
@@ -764,7 +709,7 @@ int tri_domain_get_clock(tri_domain* d, tri_clock* c) {
   c->time_increment_fixed = m->time_increment_fixed;
   c->runoff_row = m->runoff_row;
   c->src_idx_low = m->src_idx_low;
-  c->reserved = 0;
+  c->last_events = m->events;
   return TRI_OK;
 }
 

@@ -5,4 +5,6 @@ namespace tri {
 template int launch_step<float>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 template int launch_initial_dt<float>(const StepArgs&, cudaStream_t);
 template void flux_occupancy<float>(int, int*);
+template int launch_batch_step<float>(const BatchArgs&, cudaStream_t);
+template void batch_flux_occupancy<float>(int, int*);
 }  // namespace tri

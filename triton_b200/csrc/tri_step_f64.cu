@@ -5,4 +5,6 @@ namespace tri {
 template int launch_step<double>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);
 template void flux_occupancy<double>(int, int*);
+template int launch_batch_step<double>(const BatchArgs&, cudaStream_t);
+template void batch_flux_occupancy<double>(int, int*);
 }  // namespace tri

@@ -23,37 +23,6 @@
 
 namespace tri {
 
-// The bed.  FP64 form: the DEM itself.  FP32 form: per 32x32 tile an FP64
-// base level and per cell an FP32 offset from it; kernels work with bed
-// levels relative to a nearby base ('ref'), so the differences that drive the
-// flux (bed steps, water level against a neighbour's bed) keep FP32 accuracy
-// on terrain hundreds of metres high.
-template <typename T>
-struct BedMap;
-template <>
-struct BedMap<double> {
-  const double* z;
-  const double* base;  // unused
-  int ntc;
-  __device__ __forceinline__ double ref_of(int, int) const { return 0.0; }
-  __device__ __forceinline__ double local(size_t id, int, int, double) const { return z[id]; }
-  __device__ __forceinline__ double absolute(size_t id, int, int) const { return z[id]; }
-};
-template <>
-struct BedMap<float> {
-  const float* z;      // offset from the tile base
-  const double* base;  // FP64 base level of each 32x32 tile
-  int ntc;             // tiles per row
-  __device__ __forceinline__ double ref_of(int r, int c) const { return base[(r >> 5) * ntc + (c >> 5)]; }
-  __device__ __forceinline__ float local(size_t id, int r, int c, double ref) const {
-    const double b = base[(r >> 5) * ntc + (c >> 5)];
-    return b == ref ? z[id] : z[id] + (float)(b - ref);
-  }
-  __device__ __forceinline__ double absolute(size_t id, int r, int c) const {
-    return base[(r >> 5) * ntc + (c >> 5)] + (double)z[id];
-  }
-};
-
 template <typename T>
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -64,11 +33,11 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ---------------------------------------------------------------------------
 // k_clock: the per-step scalar work of the reference host loop.
 // ---------------------------------------------------------------------------
-static __global__ void k_clock(DevClock* __restrict__ c) {
-  if (threadIdx.x != 0) return;
+// Returns true when this step raised an event (the domain halts after it).
+__device__ __forceinline__ bool clock_step(DevClock* __restrict__ c) {
   if (c->halt) {
     c->active = 0;
-    return;
+    return false;
   }
   const double t0 = c->simtime;
   double dt;
@@ -125,11 +94,17 @@ static __global__ void k_clock(DevClock* __restrict__ c) {
   if (c->time_series && t1 - c->last_obs_time >= c->print_observation) ev |= TRI_EV_OBS;
   if (t1 >= c->print_interval * (c->print_id + 1)) ev |= TRI_EV_PRINT;
   if (!(t1 < c->sim_duration)) ev |= TRI_EV_END;
+  c->active = 1;
   if (ev) {
     c->halt = 1;
     c->events = ev;
+    return true;
   }
-  c->active = 1;
+  return false;
+}
+
+static __global__ void k_clock(DevClock* __restrict__ c) {
+  if (threadIdx.x == 0) clock_step(c);
 }
 
 // ---------------------------------------------------------------------------
@@ -202,156 +177,208 @@ __device__ __forceinline__ T shfl_down1(T v) {
 }
 
 
+// Everything one tile of the flux kernel needs: the domain's arrays and the
+// running step's constants (from its clock).
+template <typename T>
+struct FluxCtx {
+  DevClock* clk;
+  const T* hi;
+  const T* qxi;
+  const T* qyi;
+  T* ho;
+  T* qxo;
+  T* qyo;
+  BedMap<T> bed;
+  const T* n2;
+  const int32_t* zone;
+  const T* rates;
+  int rows, cols, rb, nstrips;
+  int nroff, roff_rows, roff_row;
+  StepK<T> K;
+};
+
+template <typename T>
+__device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>& sb, const BedMap<T>& bed,
+                                               const T* n2, const int32_t* zone, const T* rates, int rows, int cols,
+                                               int rb, T dx, T rdx, T hextra) {
+  FluxCtx<T> X;
+  X.clk = clk;
+  const int src = clk->src, dst = clk->dst;
+  X.hi = sb.h[src];
+  X.qxi = sb.qx[src];
+  X.qyi = sb.qy[src];
+  X.ho = sb.h[dst];
+  X.qxo = sb.qx[dst];
+  X.qyo = sb.qy[dst];
+  X.bed = bed;
+  X.n2 = n2;
+  X.zone = zone;
+  X.rates = rates;
+  X.rows = rows;
+  X.cols = cols;
+  X.rb = rb;
+  X.nstrips = (cols - 2 + kStripCols - 1) / kStripCols;
+  X.nroff = clk->nroff;
+  X.roff_rows = clk->roff_rows;
+  X.roff_row = clk->runoff_row;
+  X.K.dx = dx;
+  X.K.dt = T(clk->global_dt);
+  X.K.rdx = rdx;
+  X.K.rdt = T(clk->rdt);
+  X.K.hextra = hextra;
+  return X;
+}
+
+// One warp tile: strip sx (30 interior columns), rows r0..r1.
+template <typename T>
+__device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, int lane) {
+  const int rows = X.rows, cols = X.cols, rb = X.rb;
+  const T dt = X.K.dt, hextra = X.K.hextra;
+  const T* __restrict__ hi = X.hi;
+  const T* __restrict__ qxi = X.qxi;
+  const T* __restrict__ qyi = X.qyi;
+  T* __restrict__ ho = X.ho;
+  T* __restrict__ qxo = X.qxo;
+  T* __restrict__ qyo = X.qyo;
+  const int sx = (int)(tile % X.nstrips), ry = (int)(tile / X.nstrips);
+  const int c = sx * kStripCols + lane;  // = c0 - 1 + lane with c0 = 1 + 30*sx
+  const int r0 = 1 + ry * rb;
+  const int r1 = min(r0 + rb - 1, rows - 2);
+  const bool incol = c < cols;
+  const bool mid = (lane >= 1 && lane <= kStripCols);
+  const bool upd = mid && c >= 1 && c <= cols - 2;
+  const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this lane
+  const bool owner = incol && (mid || gcol);
+  constexpr bool kAcct = sizeof(T) == 4;  // FP32 form keeps the FP64 volume accounts
+  double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
+  // bed levels relative to the base of the tile's first cell
+  const double zref = X.bed.ref_of(r0, min(sx * kStripCols + 1, cols - 1));
+
+  auto copy_ghost = [&](int r) {
+    const size_t id = (size_t)r * cols + c;
+    ho[id] = hi[id];
+    qxo[id] = qxi[id];
+    qyo[id] = qyi[id];
+  };
+
+  // raw values of the next row are loaded one iteration ahead
+  T lh = T(0), lqx = T(0), lqy = T(0), lz = T(0);
+  auto fetch = [&](int r) {
+    if (incol) {
+      const size_t id = (size_t)r * cols + c;
+      lh = hi[id];
+      lqx = qxi[id];
+      lqy = qyi[id];
+      lz = X.bed.local(id, r, c, zref);
+    }
+  };
+  fetch(r0 - 1);
+  CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra);
+  if (r0 - 1 == 0 && owner) copy_ghost(0);
+  fetch(r0);
+  RowParts<T> pp;
+  pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
+  T pn2 = T(0);  // Manning of the previous row's cell
+
+  for (int r = r0; r <= r1 + 1; ++r) {
+    const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra);
+    T cn2 = T(0);
+    if (r <= r1) {
+      if (upd) cn2 = X.n2[(size_t)r * cols + c];
+      fetch(r + 1);  // r1 + 1 <= rows - 1
+    }
+    FaceOut<T> Y;
+    Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
+    if (upd) Y = face_flux<T, false>(cur, prev, X.K);
+    if (r - 1 >= r0 && upd) {
+      const size_t id = (size_t)(r - 1) * cols + c;
+      T hn, qn, vn;
+      update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn);
+      if (kAcct) {
+        // Inflow through faces shared with ghost cells, in depth units.  The
+        // update is in fluctuation form, so the mass flux through a face of
+        // boundary cell i is F(Q_i).n plus the fluctuation it receives there:
+        // west / south faces dt/dx*q - b, east / north faces -(a + dt/dx*q).
+        // Also the depth the update clipped back to zero.
+        const double sxq = (double)dt / (double)X.K.dx;
+        if (c == 1) acc_b += sxq * (double)prev.qx - (double)pp.w0;
+        if (c == cols - 2) acc_b -= (double)pp.e0 + sxq * (double)prev.qx;
+        if (r - 1 == 1) acc_b -= (double)pp.n0 + sxq * (double)prev.qy;
+        if (r - 1 == rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
+        const T raw = prev.h - (pp.e0 + pp.n0) - (pp.w0 + Y.b0);
+        if (raw < T(0)) acc_c -= (double)raw;
+      }
+      if (X.nroff > 0) {  // update_runoff (kernels.h:128-149)
+        const T h0 = hn;
+        const T net = X.rates[(size_t)X.zone[id] * X.roff_rows + X.roff_row];
+        hn += net * dt;
+        if (hn < hextra) {
+          if (hn < T(0)) hn = T(0);
+          qn = T(0);
+          vn = T(0);
+        }
+        if (kAcct) acc_r += (double)hn - (double)h0;
+      }
+      ho[id] = hn;
+      qxo[id] = qn;
+      qyo[id] = vn;
+    }
+    if (r > r1) {
+      if (r == rows - 1 && owner) copy_ghost(r);
+      break;
+    }
+    // x faces of row r: lane l evaluates the face between lanes l-1 and l
+    CellQ<T> left;
+    left.h = shfl_up1(cur.h);
+    left.qx = shfl_up1(cur.qx);
+    left.qy = shfl_up1(cur.qy);
+    left.z = shfl_up1(cur.z);
+    left.sq = shfl_up1(cur.sq);
+    left.u = shfl_up1(cur.u);
+    left.v = shfl_up1(cur.v);
+    FaceOut<T> Xf;
+    Xf.a0 = Xf.a1 = Xf.a2 = Xf.b0 = Xf.b1 = Xf.b2 = T(0);
+    if (lane >= 1 && incol && c >= 1) Xf = face_flux<T, true>(left, cur, X.K);
+    pp.e0 = shfl_down1(Xf.a0);
+    pp.e1 = shfl_down1(Xf.a1);
+    pp.e2 = shfl_down1(Xf.a2);
+    pp.w0 = Xf.b0;
+    pp.w1 = Xf.b1;
+    pp.w2 = Xf.b2;
+    pp.n0 = Y.a0;
+    pp.n1 = Y.a1;
+    pp.n2 = Y.a2;
+    pn2 = cn2;
+    if (gcol) copy_ghost(r);
+    prev = cur;
+  }
+  if (kAcct) {
+    acc_b = warp_sum<T>(acc_b);
+    acc_r = warp_sum<T>(acc_r);
+    acc_c = warp_sum<T>(acc_c);
+    if (lane == 0) {
+      if (acc_b != 0.0) atomicAdd(&X.clk->acc_step[kAccBoundary], acc_b);
+      if (acc_r != 0.0) atomicAdd(&X.clk->acc_step[kAccRunoff], acc_r);
+      if (acc_c != 0.0) atomicAdd(&X.clk->acc_step[kAccClip], acc_c);
+    }
+  }
+}
+
 template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                      const BedMap<T> bed, const T* __restrict__ n2,
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
                                                      int rows, int cols, int rb, T dx, T rdx, T hextra) {
   if (!clk->active) return;
-  const int src = clk->src, dst = clk->dst;
-  const T dt = T(clk->global_dt);
-  StepK<T> K;
-  K.dx = dx;
-  K.dt = dt;
-  K.rdx = rdx;
-  K.rdt = T(clk->rdt);
-  K.hextra = hextra;
-  const int nroff = clk->nroff, roff_rows = clk->roff_rows, roff_row = clk->runoff_row;
-  const T* __restrict__ hi = sb.h[src];
-  const T* __restrict__ qxi = sb.qx[src];
-  const T* __restrict__ qyi = sb.qy[src];
-  T* __restrict__ ho = sb.h[dst];
-  T* __restrict__ qxo = sb.qx[dst];
-  T* __restrict__ qyo = sb.qy[dst];
-
+  const FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
   const int lane = threadIdx.x & 31;
-  const int nstrips = (cols - 2 + kStripCols - 1) / kStripCols;
-  const int nrowb = (rows - 2 + rb - 1) / rb;
-  const unsigned ntiles = (unsigned)nstrips * (unsigned)nrowb;
-
+  const unsigned ntiles = (unsigned)X.nstrips * (unsigned)((rows - 2 + rb - 1) / rb);
   while (true) {
     unsigned tile = 0;
     if (lane == 0) tile = atomicAdd(&clk->tile_next, 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
-    const int sx = (int)(tile % nstrips), ry = (int)(tile / nstrips);
-    const int c = sx * kStripCols + lane;  // = c0 - 1 + lane with c0 = 1 + 30*sx
-    const int r0 = 1 + ry * rb;
-    const int r1 = min(r0 + rb - 1, rows - 2);
-    const bool incol = c < cols;
-    const bool mid = (lane >= 1 && lane <= kStripCols);
-    const bool upd = mid && c >= 1 && c <= cols - 2;
-    const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this lane
-    const bool owner = incol && (mid || gcol);
-    constexpr bool kAcct = sizeof(T) == 4;  // FP32 form keeps the FP64 volume accounts
-    double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
-    // bed levels relative to the base of the tile's first cell
-    const double zref = bed.ref_of(r0, min(sx * kStripCols + 1, cols - 1));
-
-    auto copy_ghost = [&](int r) {
-      const size_t id = (size_t)r * cols + c;
-      ho[id] = hi[id];
-      qxo[id] = qxi[id];
-      qyo[id] = qyi[id];
-    };
-
-    // raw values of the next row are loaded one iteration ahead
-    T lh = T(0), lqx = T(0), lqy = T(0), lz = T(0);
-    auto fetch = [&](int r) {
-      if (incol) {
-        const size_t id = (size_t)r * cols + c;
-        lh = hi[id];
-        lqx = qxi[id];
-        lqy = qyi[id];
-        lz = bed.local(id, r, c, zref);
-      }
-    };
-    fetch(r0 - 1);
-    CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra);
-    if (r0 - 1 == 0 && owner) copy_ghost(0);
-    fetch(r0);
-    RowParts<T> pp;
-    pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
-    T pn2 = T(0);  // Manning of the previous row's cell
-
-    for (int r = r0; r <= r1 + 1; ++r) {
-      const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra);
-      T cn2 = T(0);
-      if (r <= r1) {
-        if (upd) cn2 = n2[(size_t)r * cols + c];
-        fetch(r + 1);  // r1 + 1 <= rows - 1
-      }
-      FaceOut<T> Y;
-      Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
-      if (upd) Y = face_flux<T, false>(cur, prev, K);
-      if (r - 1 >= r0 && upd) {
-        const size_t id = (size_t)(r - 1) * cols + c;
-        T hn, qn, vn;
-        update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn);
-        if (kAcct) {
-          // inflow through faces shared with ghost cells (depth units), and
-          // the depth the update clipped back to zero
-          if (c == 1) acc_b -= (double)pp.w0;
-          if (c == cols - 2) acc_b -= (double)pp.e0;
-          if (r - 1 == 1) acc_b -= (double)pp.n0;
-          if (r - 1 == rows - 2) acc_b -= (double)Y.b0;
-          const T raw = prev.h - (pp.e0 + pp.n0) - (pp.w0 + Y.b0);
-          if (raw < T(0)) acc_c -= (double)raw;
-        }
-        if (nroff > 0) {  // update_runoff (kernels.h:128-149)
-          const T h0 = hn;
-          const T net = rates[(size_t)zone[id] * roff_rows + roff_row];
-          hn += net * dt;
-          if (hn < hextra) {
-            if (hn < T(0)) hn = T(0);
-            qn = T(0);
-            vn = T(0);
-          }
-          if (kAcct) acc_r += (double)hn - (double)h0;
-        }
-        ho[id] = hn;
-        qxo[id] = qn;
-        qyo[id] = vn;
-      }
-      if (r > r1) {
-        if (r == rows - 1 && owner) copy_ghost(r);
-        break;
-      }
-      // x faces of row r: lane l evaluates the face between lanes l-1 and l
-      CellQ<T> left;
-      left.h = shfl_up1(cur.h);
-      left.qx = shfl_up1(cur.qx);
-      left.qy = shfl_up1(cur.qy);
-      left.z = shfl_up1(cur.z);
-      left.sq = shfl_up1(cur.sq);
-      left.u = shfl_up1(cur.u);
-      left.v = shfl_up1(cur.v);
-      FaceOut<T> X;
-      X.a0 = X.a1 = X.a2 = X.b0 = X.b1 = X.b2 = T(0);
-      if (lane >= 1 && incol && c >= 1) X = face_flux<T, true>(left, cur, K);
-      pp.e0 = shfl_down1(X.a0);
-      pp.e1 = shfl_down1(X.a1);
-      pp.e2 = shfl_down1(X.a2);
-      pp.w0 = X.b0;
-      pp.w1 = X.b1;
-      pp.w2 = X.b2;
-      pp.n0 = Y.a0;
-      pp.n1 = Y.a1;
-      pp.n2 = Y.a2;
-      pn2 = cn2;
-      if (gcol) copy_ghost(r);
-      prev = cur;
-    }
-    if (kAcct) {
-      acc_b = warp_sum<T>(acc_b);
-      acc_r = warp_sum<T>(acc_r);
-      acc_c = warp_sum<T>(acc_c);
-      if (lane == 0) {
-        if (acc_b != 0.0) atomicAdd(&clk->acc_step[kAccBoundary], acc_b);
-        if (acc_r != 0.0) atomicAdd(&clk->acc_step[kAccRunoff], acc_r);
-        if (acc_c != 0.0) atomicAdd(&clk->acc_step[kAccClip], acc_c);
-      }
-    }
+    flux_tile<T>(X, tile, lane);
   }
 }
 
@@ -422,15 +449,13 @@ __global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int
   }
 }
 
+// compute_extbc_values for one boundary cell (kernels.h:254-420), single rank.
 template <typename T>
-__global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMap<T> bed,
-                        const T* __restrict__ n2, const int32_t* __restrict__ order, int count,
-                        const int32_t* __restrict__ cells, const int32_t* __restrict__ types,
-                        const int32_t* __restrict__ start, const int32_t* __restrict__ nrowsv,
-                        const T* __restrict__ var1, const T* __restrict__ var2, int rows, int cols) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= count || !clk->active) return;
-  const int id = order[k];
+__device__ __forceinline__ void extbc_apply(DevClock* __restrict__ clk, const StateBufs<T>& sb, const BedMap<T>& bed,
+                                            const T* __restrict__ n2, int id, const int32_t* __restrict__ cells,
+                                            const int32_t* __restrict__ types, const int32_t* __restrict__ start,
+                                            const int32_t* __restrict__ nrowsv, const T* __restrict__ var1,
+                                            const T* __restrict__ var2, int rows, int cols) {
   const int d = clk->dst;
   T* h = sb.h[d];
   T* qx = sb.qx[d];
@@ -551,6 +576,17 @@ __global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMa
   }
 }
 
+template <typename T>
+__global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMap<T> bed, const T* __restrict__ n2,
+                        const int32_t* __restrict__ order, int count, const int32_t* __restrict__ cells,
+                        const int32_t* __restrict__ types, const int32_t* __restrict__ start,
+                        const int32_t* __restrict__ nrowsv, const T* __restrict__ var1, const T* __restrict__ var2,
+                        int rows, int cols) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count || !clk->active) return;
+  extbc_apply<T>(clk, sb, bed, n2, order[k], cells, types, start, nrowsv, var1, var2, rows, cols);
+}
+
 // ---------------------------------------------------------------------------
 // k_wetdry_dt: wet/dry masks and max depth on interior cells, then the CFL dt
 // of every cell (ghosts included, as compute_dt_and_sqrt runs over rows*cols)
@@ -561,35 +597,37 @@ __global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMa
 // iteration ahead; east/west neighbours come by shuffle (lanes 0 and 31 load
 // theirs).  Every value is read once, with several loads in flight.
 // ---------------------------------------------------------------------------
-template <typename T, bool WETDRY>
-__global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
-                                                        const BedMap<T> bed, T* __restrict__ maxh, int rows,
-                                                        int cols, int band, double dx, double cn, T hextra,
-                                                        float* __restrict__ arrival, float arrival_depth) {
-  if (WETDRY && !clk->active) return;
-  if (sizeof(T) == 4 && WETDRY && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-    // fold this step's volume terms into the Kahan-compensated totals
-    for (int k = 0; k < kAccTerms; k++) {
-      const double y = clk->acc_step[k] - clk->acc_comp[k];
-      const double t = clk->acc_sum[k] + y;
-      clk->acc_comp[k] = (t - clk->acc_sum[k]) - y;
-      clk->acc_sum[k] = t;
-      clk->acc_step[k] = 0.0;
-    }
+// Kahan fold of the step's volume terms into the domain's totals.
+__device__ __forceinline__ void fold_accounts(DevClock* __restrict__ clk) {
+  for (int k = 0; k < kAccTerms; k++) {
+    const double y = clk->acc_step[k] - clk->acc_comp[k];
+    const double t = clk->acc_sum[k] + y;
+    clk->acc_comp[k] = (t - clk->acc_sum[k]) - y;
+    clk->acc_sum[k] = t;
+    clk->acc_step[k] = 0.0;
   }
+}
+
+// One block's band: columns bx*128 .. +127, rows by*band .. +band-1.
+// Returns this thread's minimum dt key.
+template <typename T, bool WETDRY>
+__device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __restrict__ clk, const StateBufs<T>& sb,
+                                                          const BedMap<T>& bed, T* __restrict__ maxh, int rows,
+                                                          int cols, int band, double dx, double cn, T hextra,
+                                                          float* __restrict__ arrival, float arrival_depth, int bx,
+                                                          int by) {
   const int buf = WETDRY ? clk->dst : clk->cur;
-  const int slot = WETDRY ? clk->wr : clk->rd;
   const T* __restrict__ h = sb.h[buf];
   T* __restrict__ qx = sb.qx[buf];
   T* __restrict__ qy = sb.qy[buf];
   const T E12 = eps12<T>();
   const int lane = threadIdx.x & 31;
-  const int c = blockIdx.x * kWetCols + threadIdx.x;
-  const int ra = blockIdx.y * band;
+  const int c = bx * kWetCols + threadIdx.x;
+  const int ra = by * band;
   const int rz = min(ra + band - 1, rows - 1);
   const bool incol = c < cols;
   const bool intcol = c >= 1 && c <= cols - 2;
-  const double zref = bed.ref_of(ra, min(blockIdx.x * kWetCols, cols - 1));
+  const double zref = bed.ref_of(ra, min(bx * kWetCols, cols - 1));
   const float simtime_now = WETDRY ? (float)clk->simtime : 0.0f;
 
   T hm = T(0), zm = T(0), h0 = T(0), z0 = T(0), hp = T(0), zp = T(0);
@@ -660,21 +698,137 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
     qy0 = qyp;
     mh0 = mhp;
   }
-  // warp -> block -> device minimum
+  return key;
+}
+
+// Block minimum of the threads' keys, folded into *slot with one atomic.
+__device__ __forceinline__ void block_min_into(unsigned long long key, unsigned long long* slot) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
     key = other < key ? other : key;
   }
   __shared__ unsigned long long s_min[kWetCols / 32];
-  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) s_min[warp] = key;
   __syncthreads();
   if (threadIdx.x == 0) {
     key = s_min[0];
     for (int w = 1; w < kWetCols / 32; w++) key = s_min[w] < key ? s_min[w] : key;
-    if (key < kDtKeyInf) atomicMin(&clk->dt_key[slot], key);
+    if (key < kDtKeyInf) atomicMin(slot, key);
   }
+}
+
+template <typename T, bool WETDRY>
+__global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                        const BedMap<T> bed, T* __restrict__ maxh, int rows,
+                                                        int cols, int band, double dx, double cn, T hextra,
+                                                        float* __restrict__ arrival, float arrival_depth) {
+  if (WETDRY && !clk->active) return;
+  if (sizeof(T) == 4 && WETDRY && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  const unsigned long long key = wetdry_band<T, WETDRY>(clk, sb, bed, maxh, rows, cols, band, dx, cn, hextra,
+                                                        arrival, arrival_depth, blockIdx.x, blockIdx.y);
+  block_min_into(key, &clk->dt_key[WETDRY ? clk->wr : clk->rd]);
+}
+
+// ===========================================================================
+// Batched ensembles: one launch per kernel type advances every member of a
+// batch by one of its own steps (each member keeps its own clock and dt).
+// Members are described in device memory (MemberDev); the flux kernel's warps
+// take tiles from one queue over all members' tiles, the wet-dry kernel's
+// blocks are a concatenation of every member's bands.
+// ===========================================================================
+template <typename T>
+__device__ __forceinline__ int member_of(const MemberDev<T>* __restrict__ mem, int nm, uint32_t x, bool tiles) {
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const uint32_t b = tiles ? mem[mid].tile_begin : mem[mid].wet_begin;
+    if (b <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__global__ void k_batch_clock(const MemberDev<T>* __restrict__ mem, int nm, BatchCtl* __restrict__ ctl) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0) ctl->tile_next = 0;
+  if (m < nm && clock_step(mem[m].clk)) atomicAdd(&ctl->halted, 1);
+}
+
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __restrict__ mem, int nm,
+                                                          BatchCtl* __restrict__ ctl, uint32_t ntiles) {
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(&ctl->tile_next, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= ntiles) break;
+    const int m = member_of<T>(mem, nm, tile, true);
+    const MemberDev<T>& M = mem[m];
+    if (!M.clk->active) continue;
+    const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
+                                     M.hextra);
+    flux_tile<T>(X, tile - M.tile_begin, lane);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* __restrict__ mem, int nm) {
+  const int m = member_of<T>(mem, nm, blockIdx.x, false);
+  const MemberDev<T>& M = mem[m];
+  DevClock* clk = M.clk;
+  if (!clk->active) return;
+  const uint32_t local = blockIdx.x - M.wet_begin;
+  if (sizeof(T) == 4 && local == 0 && threadIdx.x == 0) fold_accounts(clk);
+  const unsigned long long key =
+      wetdry_band<T, true>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, kWetBand, M.dxd, M.courant, M.hextra, M.arrival,
+                           M.arrival_depth, (int)(local % M.wet_nbx), (int)(local / M.wet_nbx));
+  block_min_into(key, &clk->dt_key[clk->wr]);
+}
+
+// Sparse forcing of a batch: items are (member, index) pairs of one
+// conflict-free wave (a member's own waves keep its index order).
+template <typename T>
+__global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2* __restrict__ items, int count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int m = items[k].x, id = items[k].y;
+  const MemberDev<T>& M = mem[m];
+  DevClock* clk = M.clk;
+  if (!clk->active) return;
+  const int lo = clk->src_idx_low, hi = clk->src_idx_high;
+  const T dt = T(clk->global_dt), simtime = T(clk->t_step);
+  T* h = M.sb.h[clk->dst];
+  const T flo = M.hyg_v[(size_t)lo * M.nsrc + id], fhi = M.hyg_v[(size_t)hi * M.nsrc + id];
+  const T tlo = T(M.hyg_t[lo]), thi = T(M.hyg_t[hi]);
+  T flow;
+  if (lo == hi) {
+    flow = flo;
+  } else {
+    const T td = simtime - tlo, td2 = thi - tlo;
+    flow = flo + (((fhi - flo) * td) / td2);
+  }
+  const int sid = M.src_cells[id];
+  T hij = h[sid];
+  const T hs = (flow * dt) / (M.dx * M.dx);
+  hij += hs;
+  h[sid] = hij;
+  if (sizeof(T) == 4) atomicAdd(&clk->acc_step[kAccSources], (double)hs);
+}
+
+template <typename T>
+__global__ void k_batch_extbc(const MemberDev<T>* __restrict__ mem, const int2* __restrict__ items, int count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const MemberDev<T>& M = mem[items[k].x];
+  if (!M.clk->active) return;
+  extbc_apply<T>(M.clk, M.sb, M.bed, M.n2, items[k].y, M.bc_cells, M.bc_types, M.bc_start, M.bc_nrows, M.bc_v1,
+                 M.bc_v2, M.rows, M.cols);
 }
 
 }  // namespace tri

@@ -59,11 +59,35 @@ int launch_initial_dt(const StepArgs& a, cudaStream_t s);
 template <typename T>
 void flux_occupancy(int variant, int* per_sm);
 
+// A batch of member domains advanced together (one step of each member per
+// batched step).  Device pointers; wave offsets are host arrays.
+struct BatchArgs {
+  const void* mem;  // MemberDev<T>[nm] in device memory
+  int nm;
+  BatchCtl* ctl;
+  uint32_t ntiles, nwet_blocks;
+  int flux_blocks, flux_variant;
+  const int2* src_items;
+  const int32_t* src_waves;
+  int n_src_waves;
+  const int2* bc_items;
+  const int32_t* bc_waves;
+  int n_bc_waves;
+};
+template <typename T>
+int launch_batch_step(const BatchArgs& a, cudaStream_t s);
+template <typename T>
+void batch_flux_occupancy(int variant, int* per_sm);
+
 extern template int launch_step<double>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 extern template int launch_step<float>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 extern template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);
 extern template int launch_initial_dt<float>(const StepArgs&, cudaStream_t);
 extern template void flux_occupancy<double>(int, int*);
 extern template void flux_occupancy<float>(int, int*);
+extern template int launch_batch_step<double>(const BatchArgs&, cudaStream_t);
+extern template int launch_batch_step<float>(const BatchArgs&, cudaStream_t);
+extern template void batch_flux_occupancy<double>(int, int*);
+extern template void batch_flux_occupancy<float>(int, int*);
 
 }  // namespace tri

@@ -46,4 +46,65 @@ struct StateBufs {
   T* qy[2];
 };
 
+// The bed.  FP64 form: the DEM itself.  FP32 form: per 32x32 tile an FP64
+// base level and per cell an FP32 offset from it; kernels work with bed
+// levels relative to a nearby base ('ref'), so the differences that drive the
+// flux (bed steps, water level against a neighbour's bed) keep FP32 accuracy
+// on terrain hundreds of metres high.
+template <typename T>
+struct BedMap;
+template <>
+struct BedMap<double> {
+  const double* z;
+  const double* base;  // unused
+  int ntc;
+  __device__ __forceinline__ double ref_of(int, int) const { return 0.0; }
+  __device__ __forceinline__ double local(size_t id, int, int, double) const { return z[id]; }
+  __device__ __forceinline__ double absolute(size_t id, int, int) const { return z[id]; }
+};
+template <>
+struct BedMap<float> {
+  const float* z;      // offset from the tile base
+  const double* base;  // FP64 base level of each 32x32 tile
+  int ntc;             // tiles per row
+  __device__ __forceinline__ double ref_of(int r, int c) const { return base[(r >> 5) * ntc + (c >> 5)]; }
+  __device__ __forceinline__ float local(size_t id, int r, int c, double ref) const {
+    const double b = base[(r >> 5) * ntc + (c >> 5)];
+    return b == ref ? z[id] : z[id] + (float)(b - ref);
+  }
+  __device__ __forceinline__ double absolute(size_t id, int r, int c) const {
+    return base[(r >> 5) * ntc + (c >> 5)] + (double)z[id];
+  }
+};
+
+template <typename T>
+struct MemberDev {
+  DevClock* clk;
+  StateBufs<T> sb;
+  BedMap<T> bed;
+  const T* n2;
+  const int32_t* zone;
+  const T* rates;
+  T* maxh;
+  float* arrival;
+  float arrival_depth;
+  int rows, cols, rb;
+  T dx, rdx, hextra;
+  double dxd, courant;
+  uint32_t tile_begin, tile_end;  // this member's tiles in the flux queue
+  uint32_t wet_begin, wet_nbx;    // first wet-dry block, blocks per band row
+  // sparse forcing (device arrays of the member)
+  int nsrc;
+  const int32_t* src_cells;
+  const double* hyg_t;
+  const T* hyg_v;
+  const int32_t *bc_cells, *bc_types, *bc_start, *bc_nrows;
+  const T *bc_v1, *bc_v2;
+};
+
+struct BatchCtl {
+  uint32_t tile_next;  // flux tile queue, reset every batched step
+  int32_t halted;      // members that raised an event during this advance call
+};
+
 }  // namespace tri

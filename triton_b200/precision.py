@@ -46,6 +46,7 @@ def compare(sc, duration=None, arrival_depth=0.1):
     b = run_form(sc, "fp32", duration, arrival_depth)
     ha, hb = a["h"][1:-1, 1:-1], b["h"][1:-1, 1:-1]
     err = np.abs(hb - ha)
+    worst = np.unravel_index(int(np.argmax(err)), err.shape)
     ta, tb = a["arrival"][1:-1, 1:-1], b["arrival"][1:-1, 1:-1]
     both = (ta >= 0) & (tb >= 0)
     terr = np.abs(tb[both] - ta[both])
@@ -55,6 +56,8 @@ def compare(sc, duration=None, arrival_depth=0.1):
     return dict(
         steps_fp64=a["steps"], steps_fp32=b["steps"], simtime=a["simtime"],
         max_depth_error_m=float(err.max()), rms_depth_error_m=float(np.sqrt(np.mean(err ** 2))),
+        cells_over_1mm=int((err > 1e-3).sum()), worst_cell=tuple(int(i) + 1 for i in worst),
+        worst_h_fp64=float(ha[worst]), worst_h_fp32=float(hb[worst]),
         arrival_max_error_s=float(terr.max()) if terr.size else 0.0,
         arrival_rms_error_s=float(np.sqrt(np.mean(terr ** 2))) if terr.size else 0.0,
         arrival_cells=int(both.sum()), arrival_mismatch_cells=int(((ta >= 0) != (tb >= 0)).sum()),

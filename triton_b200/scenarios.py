@@ -232,17 +232,41 @@ def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, r
     sc = Scenario("watershed", dx, z, zero.copy(), zero.copy(), zero.copy(), n2, courant=0.5, hextra=0.001,
                   sim_duration=duration, print_interval=pi, meta=dict(n=n, seed=seed, mann=mann))
     # inflows along the valley in the northern half: 0 -> peak at 2 h -> 0 at 4 h
-    src_rows = np.linspace(n * 0.1, n * 0.45, nsrc).astype(int)
-    src_cols = (n / 2 + 0.15 * n * np.sin(2 * np.pi * src_rows / (0.6 * n))).astype(int)
-    flows = np.zeros((4, nsrc))
-    flows[1, :] = peak_flow
-    sources_table(sc, list(zip(src_rows.tolist(), src_cols.tolist())), [0.0, 2.0, 4.0, 1000.0], flows)
+    if nsrc > 0:
+        src_rows = np.linspace(n * 0.1, n * 0.45, nsrc).astype(int)
+        src_cols = (n / 2 + 0.15 * n * np.sin(2 * np.pi * src_rows / (0.6 * n))).astype(int)
+        flows = np.zeros((4, nsrc))
+        flows[1, :] = peak_flow
+        sources_table(sc, list(zip(src_rows.tolist(), src_cols.tolist())), [0.0, 2.0, 4.0, 1000.0], flows)
     # uniform rain on one zone: (0 h, rain), (rain_hours, 0), (end, 0)
     end_h = max(duration / 3600.0, rain_hours + 1.0)
     runoff_table(sc, np.zeros((n, n), dtype=np.int32), [0.0, rain_hours, end_h], [[rain_mm_h], [0.0], [0.0]])
     # open outflow (type 0) along the southern edge, the lowest one
     extbc_segments(sc, [(0, (n - 1, 0), (n - 1, n - 1), None)])
     return sc
+
+
+def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0, 20.0), duration=3 * 3600.0,
+             rain_range=(10.0, 100.0), rain_hours=1.0, manning_spread=0.3, max_side=None):
+    """Ensemble of rain-on-grid watershed members of uneven sizes: per member
+    a side drawn log-uniformly in [side_min, side_max] (capped at max_side),
+    a cell size in dx_range, a rain intensity in rain_range (mm/h) for
+    rain_hours, a Manning median scaled by exp(N(0, manning_spread)) and its
+    own terrain seed.  Members carry no point sources."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(members):
+        side = int(np.exp(rng.uniform(np.log(side_min), np.log(side_max))))
+        if max_side is not None:
+            side = min(side, max_side)
+        dx = float(rng.uniform(*dx_range))
+        rain = float(rng.uniform(*rain_range))
+        mann = 0.035 * float(np.exp(manning_spread * rng.standard_normal()))
+        sc = watershed(n=side, dx=dx, seed=int(rng.integers(1 << 31)), duration=duration, rain_mm_h=rain,
+                       rain_hours=rain_hours, manning_median=mann, nsrc=0)
+        sc.name = f"member{i:03d}"
+        out.append(sc)
+    return out
 
 
 def extbc_segments(sc, segments):
