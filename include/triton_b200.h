@@ -274,6 +274,27 @@ int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double d
                                         const int32_t* extbctype, const int32_t* start_index,
                                         const int32_t* nrows_vars, const double* extbcvar1, const double* extbcvar2,
                                         double simtime, int rank, int total_process, void* stream);
+/* No-alloc variant of tri_kernel_compute_extbc_values_f64; it has no
+ * counterpart in the reference.  Same arguments, same results, and it also
+ * synchronizes 'stream'.  It allocates no device memory: the application
+ * order is kept in a fixed array inside the library of
+ * TRI_NOALLOC_EXTBC_MAX_CELLS entries (256 KiB), and a longer cell list is
+ * rejected with TRI_E_INVALID.  For callers that cannot allocate device
+ * memory inside their time loop: a host that claimed the GPU's free memory
+ * before the loop (a memory pool or caching allocator in the same process)
+ * would see cudaMalloc fail mid-run, and cudaMalloc/cudaFree synchronize the
+ * whole device.  The first call on each device looks up the array's address
+ * (which may load the library's device code); make it before any stream
+ * capture.  The array is shared by every call on a device: calls that
+ * overlap in time (from other host threads, or while kernels of an earlier
+ * call with another cell list still run on another stream) race on it. */
+#define TRI_NOALLOC_EXTBC_MAX_CELLS 65536
+int tri_kernel_compute_extbc_values_noalloc_f64(int size, int nrows, int ncols, double dt, double* h, double* qx,
+                                                double* qy, const double* dem, const double* n,
+                                                const int32_t* relative_index, const int32_t* extbctype,
+                                                const int32_t* start_index, const int32_t* nrows_vars,
+                                                const double* extbcvar1, const double* extbcvar2, double simtime,
+                                                int rank, int total_process, void* stream);
 int tri_kernel_wet_dry_f64(int size, int nrows, int ncols, double dt, const double* h, double* qx, double* qy,
                            const double* dem, double* max_h, double hextra, int mpi_tasks, void* stream);
 int tri_kernel_copy_observation_points_f64(int size, const double* arr, double* obs_arr,

@@ -11,6 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libtriton_b200.so")
 
+NOALLOC_EXTBC_MAX_CELLS = 65536  # TRI_NOALLOC_EXTBC_MAX_CELLS
 TRI_OK, TRI_E_INVALID, TRI_E_CUDA, TRI_E_NOMEM, TRI_E_STATE, TRI_E_IO, TRI_E_TIMEOUT = range(7)
 TRI_FP64, TRI_FP32 = 0, 1
 FIELD_H, FIELD_QX, FIELD_QY, FIELD_NMAN2, FIELD_DEM, FIELD_MAXH = range(6)
@@ -108,6 +109,8 @@ _SIGS = {
                                                                               _vp, C.c_int, C.c_int, _vp]),
     "tri_kernel_compute_extbc_values_f64": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [_vp] * 11 +
                                             [C.c_double, C.c_int, C.c_int, _vp]),
+    "tri_kernel_compute_extbc_values_noalloc_f64": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [_vp] * 11 +
+                                                    [C.c_double, C.c_int, C.c_int, _vp]),
     "tri_kernel_wet_dry_f64": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                          C.c_int, _vp]),
     "tri_kernel_copy_observation_points_f64": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp]),

@@ -5,6 +5,7 @@
 // domain path (tri_domain.cu) is the fast path.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "tri_face.cuh"
@@ -504,3 +505,84 @@ int tri_kernel_copy_observation_points_f64(int size, const double* arr, double* 
 }
 
 }  // extern "C"
+
+// ---- no-alloc variant of compute_extbc_values ------------------------------
+// tri_kernel_compute_extbc_values_f64 keeps its application order in device
+// memory it allocates (and grows) on first use.  Callers that cannot allocate
+// device memory inside their time loop use the variant below, whose order
+// lives in a fixed array in the library's own device image: a host that
+// claimed the GPU's free memory before the loop (the reference creates every
+// device array up front, triton_init.h:1452-1591; a memory pool or caching
+// allocator in the same process may hold the rest) would see cudaMalloc fail
+// mid-run, and cudaMalloc/cudaFree synchronize the whole device, stalling the
+// other streams of the step.
+namespace {
+
+// 65536 boundary cells (the four edges of a 16384 x 16384 interior), 256 KiB.
+constexpr int kNoAllocExtbcMaxCells = TRI_NOALLOC_EXTBC_MAX_CELLS;
+// Application order: indices into the cell list, wave after wave.  Nothing in
+// it has to start at zero: a call launches the boundary kernel only after the
+// order of its own cell list has been written here (by this call, or by the
+// previous call on this device with the same list).
+static __device__ __align__(256) int32_t g_extbc_order[kNoAllocExtbcMaxCells];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocSlot {
+  int32_t* order = nullptr;    // device address of g_extbc_order on this device
+  std::vector<int32_t> cells;  // cell list whose order g_extbc_order holds
+  std::vector<int32_t> order_host, waves;
+};
+std::mutex g_noalloc_mu;  // guards the host-side slots only
+NoAllocSlot g_noalloc[kNoAllocMaxDevices];
+
+}  // namespace
+
+extern "C" int tri_kernel_compute_extbc_values_noalloc_f64(
+    int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy, const double* dem, const double* n,
+    const int32_t* relative_index, const int32_t* extbctype, const int32_t* start_index, const int32_t* nrows_vars,
+    const double* extbcvar1, const double* extbcvar2, double simtime, int rank, int total_process, void* stream) {
+  if (size <= 0) return TRI_OK;
+  TRI_CHECK_ARG(size <= kNoAllocExtbcMaxCells,
+                "compute_extbc_values_noalloc: %d boundary cells exceed its fixed limit of %d; use "
+                "tri_kernel_compute_extbc_values_f64 for longer lists",
+                size, kNoAllocExtbcMaxCells);
+  TRI_CHECK_ARG(relative_index && extbctype && start_index && nrows_vars, "null device pointer");
+  int dev = 0;
+  TRI_CUDA_TRY(cudaGetDevice(&dev));
+  TRI_CHECK_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "device %d beyond the %d devices the no-alloc entry serves",
+                dev, kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocSlot& slot = g_noalloc[dev];
+  if (!slot.order) {
+    // once per device, with that device current; may load the module
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_extbc_order);
+    if (e != cudaSuccess || !p)
+      return set_error(TRI_E_CUDA, "compute_extbc_values_noalloc: address of the order array on device %d: %s",
+                       dev, cudaGetErrorString(e));
+    slot.order = (int32_t*)p;
+  }
+  cudaStream_t s = as_stream(stream);
+  std::vector<int32_t> cells((size_t)size);
+  TRI_CUDA_TRY(cudaMemcpyAsync(cells.data(), relative_index, size * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  TRI_CUDA_TRY(cudaStreamSynchronize(s));
+  if (cells != slot.cells) {
+    std::vector<std::vector<int64_t>> touch((size_t)size);
+    for (int i = 0; i < size; i++) {
+      const int64_t ii = cells[i];
+      touch[i] = {ii, ii - 1, ii + 1, ii - ncols, ii + ncols};
+    }
+    slot.cells.clear();  // stays invalid if the copy below fails
+    build_waves(touch, slot.order_host, slot.waves);
+    TRI_CUDA_TRY(cudaMemcpyAsync(slot.order, slot.order_host.data(), slot.order_host.size() * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, s));
+    slot.cells = std::move(cells);
+  }
+  for (size_t w = 0; w + 1 < slot.waves.size(); w++) {
+    const int off = slot.waves[w], cnt = slot.waves[w + 1] - off;
+    kr_extbc<<<nblocks(cnt), kThreads, 0, s>>>(slot.order + off, cnt, nrows, ncols, dt, h, qx, qy, dem, n,
+                                                relative_index, extbctype, start_index, nrows_vars, extbcvar1,
+                                                extbcvar2, simtime, rank, total_process);
+  }
+  return launched();
+}
