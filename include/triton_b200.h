@@ -225,6 +225,9 @@ typedef struct tri_batch_progress {
 /* stream: cudaStream_t for the batched launches, NULL = the batch makes one. */
 int tri_batch_create(int32_t nmembers, tri_domain* const* members, void* stream, tri_batch** out);
 int tri_batch_destroy(tri_batch* b);
+/* Replaces the member list (0 members allowed; same rules as create).  For a
+ * request loop that admits and retires domains between advances. */
+int tri_batch_set_members(tri_batch* b, int32_t nmembers, tri_domain* const* members);
 /* Advances every member until it raises an event (its clock then halts, as in
  * tri_domain_advance) or until max_steps batched steps have run.  Members
  * already at their end take no steps.  Blocks until done. */

@@ -86,6 +86,7 @@ _SIGS = {
     "tri_domain_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "tri_batch_create": (C.c_int, [C.c_int32, C.POINTER(_vp), _vp, C.POINTER(_vp)]),
     "tri_batch_destroy": (C.c_int, [_vp]),
+    "tri_batch_set_members": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp)]),
     "tri_batch_advance": (C.c_int, [_vp, C.c_int32, C.POINTER(BatchProgress)]),
     "tri_batch_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_batch_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),

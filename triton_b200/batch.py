@@ -38,6 +38,11 @@ class Batch:
     def __exit__(self, *exc):
         self.close()
 
+    def set_members(self, members):
+        self.members = list(members)
+        arr = (C.c_void_p * max(len(self.members), 1))(*[m._h for m in self.members])
+        check(lib().tri_batch_set_members(self._h, len(self.members), arr))
+
     def advance(self, max_steps):
         """Runs until every member has raised an event or max_steps batched
         steps have run; returns a BatchProgress."""

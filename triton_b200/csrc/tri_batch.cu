@@ -109,6 +109,8 @@ int build_table(tri_batch* b) {
   b->nwet = wet;
   if (b->d_mem) cudaFree(b->d_mem);
   b->d_mem = nullptr;
+  drop_graph(b);
+  if (tab.empty()) return TRI_OK;
   TRI_CUDA_TRY(cudaMalloc(&b->d_mem, tab.size() * sizeof(MemberDev<T>)));
   TRI_CUDA_TRY(cudaMemcpy(b->d_mem, tab.data(), tab.size() * sizeof(MemberDev<T>), cudaMemcpyHostToDevice));
   int sms = 148, dev = 0, per_sm = 0;
@@ -232,30 +234,38 @@ int prepare_members(tri_batch* b, int* runnable) {
   return TRI_OK;
 }
 
+// Members of one batch: existing, distinct, one precision, no open edges.
+int check_members(int prec, int32_t n, tri_domain* const* members, std::vector<tri_domain*>& out) {
+  out.clear();
+  for (int i = 0; i < n; i++) {
+    tri_domain* d = members[i];
+    if (!d || d->prec != prec || d->desc.open_boundaries)
+      return set_error(TRI_E_INVALID,
+                       "batch member %d: members must exist, share one precision and use closed or "
+                       "external-boundary edges (open_boundaries=0)",
+                       i);
+    for (int j = 0; j < i; j++)
+      if (members[j] == d) return set_error(TRI_E_INVALID, "batch member %d repeats member %d", i, j);
+    out.push_back(d);
+  }
+  return TRI_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 int tri_batch_create(int32_t nmembers, tri_domain* const* members, void* stream, tri_batch** out) {
-  TRI_CHECK_ARG(out && members && nmembers >= 1, "need at least one member");
+  TRI_CHECK_ARG(out && members && nmembers >= 1 && members[0], "need at least one member");
   *out = nullptr;
   tri_batch* b = new tri_batch();
-  b->prec = members[0] ? members[0]->prec : TRI_FP64;
-  for (int i = 0; i < nmembers; i++) {
-    tri_domain* d = members[i];
-    if (!d || d->prec != b->prec || d->desc.open_boundaries) {
+  b->prec = members[0]->prec;
+  {
+    const int rc0 = check_members(b->prec, nmembers, members, b->members);
+    if (rc0 != TRI_OK) {
       delete b;
-      return set_error(TRI_E_INVALID,
-                       "batch member %d: members must exist, share one precision and use closed or "
-                       "external-boundary edges (open_boundaries=0)",
-                       i);
+      return rc0;
     }
-    for (int j = 0; j < i; j++)
-      if (members[j] == d) {
-        delete b;
-        return set_error(TRI_E_INVALID, "batch member %d repeats member %d", i, j);
-      }
-    b->members.push_back(d);
   }
   int rc = TRI_OK;
   auto fail = [&](int code) {
@@ -298,6 +308,18 @@ int tri_batch_destroy(tri_batch* b) {
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return TRI_OK;
+}
+
+int tri_batch_set_members(tri_batch* b, int32_t nmembers, tri_domain* const* members) {
+  TRI_CHECK_ARG(b && nmembers >= 0 && (nmembers == 0 || members), "null argument");
+  std::vector<tri_domain*> next;
+  int rc = check_members(b->prec, nmembers, members, next);
+  if (rc != TRI_OK) return rc;
+  TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (tri_domain* d : next) TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  b->members = std::move(next);
+  if ((rc = rebuild(b)) != TRI_OK) return rc;
+  return build_items(b);
 }
 
 int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* p) {
@@ -356,6 +378,7 @@ int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile) {
 
 int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out) {
   TRI_CHECK_ARG(b && out, "null argument");
+  TRI_CHECK_ARG(!b->members.empty(), "autotune needs at least one member");
   TRI_CHECK_ARG(trial_steps >= 1, "trial_steps must be >= 1");
   // snapshot every member: current state, max depth and clock
   struct Snap {

@@ -626,8 +626,7 @@ int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, co
                   "extbc cell %d table rows [%d,%d) outside [0,%d)", i, start[i], start[i] + nrows[i], nvars);
     const int ix = ii / Cc, iy = ii % Cc;
     TRI_CHECK_ARG(ix >= 1 && ix <= R - 2 && iy >= 1 && iy <= Cc - 2, "extbc cell %d is not an interior cell", i);
-    // the inner cell, the ghost it writes and, at a corner, the second ghost
-    touch[i] = {ii, (int64_t)ii - 1, (int64_t)ii + 1, (int64_t)ii - Cc, (int64_t)ii + Cc};
+    touch[i] = extbc_touches(ii, R, Cc);
   }
   std::vector<int32_t> order;
   build_waves(touch, order, d->bc_waves);

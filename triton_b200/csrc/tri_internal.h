@@ -37,4 +37,19 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 void build_waves(const std::vector<std::vector<int64_t>>& touches, std::vector<int32_t>& order,
                  std::vector<int32_t>& wave_start);
 
+// Cells one external-boundary item may read or write (compute_extbc_values,
+// kernels.h:237-424): its own cell ii and the ghost next to it on every edge
+// the cell lies on (that covers the ghost it writes and, at a corner, the
+// second one).  Items on different cells never share a cell, so boundary
+// rows and columns run as one wave; only a cell listed twice is ordered.
+inline std::vector<int64_t> extbc_touches(int64_t ii, int rows, int cols) {
+  const int64_t ix = ii / cols, iy = ii % cols;
+  std::vector<int64_t> t{ii};
+  if (iy == 1) t.push_back(ii - 1);
+  if (iy == cols - 2) t.push_back(ii + 1);
+  if (ix == 1) t.push_back(ii - cols);
+  if (ix == rows - 2) t.push_back(ii + cols);
+  return t;
+}
+
 }  // namespace tri

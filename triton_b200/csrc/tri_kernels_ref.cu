@@ -468,7 +468,7 @@ int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double d
     std::vector<std::vector<int64_t>> touch((size_t)size);
     for (int i = 0; i < size; i++) {
       const int64_t ii = cells[i];
-      touch[i] = {ii, ii - 1, ii + 1, ii - ncols, ii + ncols};
+      touch[i] = extbc_touches(ii, nrows, ncols);
     }
     build_waves(touch, order, waves);
     if (d_order_cap < order.size()) {
@@ -570,7 +570,7 @@ extern "C" int tri_kernel_compute_extbc_values_noalloc_f64(
     std::vector<std::vector<int64_t>> touch((size_t)size);
     for (int i = 0; i < size; i++) {
       const int64_t ii = cells[i];
-      touch[i] = {ii, ii - 1, ii + 1, ii - ncols, ii + ncols};
+      touch[i] = extbc_touches(ii, nrows, ncols);
     }
     slot.cells.clear();  // stays invalid if the copy below fails
     build_waves(touch, slot.order_host, slot.waves);

@@ -251,8 +251,8 @@ def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0,
     """Ensemble of rain-on-grid watershed members of uneven sizes: per member
     a side drawn log-uniformly in [side_min, side_max] (capped at max_side),
     a cell size in dx_range, a rain intensity in rain_range (mm/h) for
-    rain_hours, a Manning median scaled by exp(N(0, manning_spread)) and its
-    own terrain seed.  Members carry no point sources."""
+    rain_hours, the Manning median 0.035 perturbed uniformly by
+    +/- manning_spread (relative) and its own terrain seed.  Members carry no point sources."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(members):
@@ -261,7 +261,7 @@ def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0,
             side = min(side, max_side)
         dx = float(rng.uniform(*dx_range))
         rain = float(rng.uniform(*rain_range))
-        mann = 0.035 * float(np.exp(manning_spread * rng.standard_normal()))
+        mann = 0.035 * (1.0 + float(rng.uniform(-manning_spread, manning_spread)))
         sc = watershed(n=side, dx=dx, seed=int(rng.integers(1 << 31)), duration=duration, rain_mm_h=rain,
                        rain_hours=rain_hours, manning_median=mann, nsrc=0)
         sc.name = f"member{i:03d}"
