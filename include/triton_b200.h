@@ -199,9 +199,11 @@ int tri_domain_get_tuning(tri_domain* d, tri_tuning* out);
 /* Sets the flux kernel's launch shape directly (variant 0..2, rows per tile >= 1). */
 int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile);
 
-/* Self-check of the exact division by a reused divisor used in the kernels:
- * n pseudo-random (a, b) pairs from 'seed' over the magnitudes the step
- * produces; counts quotients that differ in any bit from IEEE a/b. */
+/* Self-check of the exact divisions by a reused divisor used in the kernels:
+ * for each of n pseudo-random indices from 'seed', one (a, b) pair over the
+ * magnitudes the step produces and one over all finite dividends (subnormals
+ * and signed zeros included) and divisors 1e-30 .. 1e30; counts quotients
+ * that differ in any bit from IEEE a/b. */
 int tri_selftest_division(int64_t n, uint64_t seed, int64_t* mismatches);
 
 /* ---- batches of member domains ------------------------------------------ */
@@ -232,6 +234,13 @@ int tri_batch_set_members(tri_batch* b, int32_t nmembers, tri_domain* const* mem
  * tri_domain_advance) or until max_steps batched steps have run.  Members
  * already at their end take no steps.  Blocks until done. */
 int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* out);
+/* Split form for a host loop that works while the GPU steps: launch queues
+ * 'steps' batched steps and returns at once (members that end or raise an
+ * event halt on the device and idle for the rest); wait blocks until they are
+ * done and reads the members' clocks.  Between the two, the members and the
+ * batch must not be touched; other batches may launch. */
+int tri_batch_launch(tri_batch* b, int32_t steps);
+int tri_batch_wait(tri_batch* b, tri_batch_progress* out);
 /* Launch-shape autotuner of the batched flux kernel; members' states, maximum
  * depths and clocks are restored afterwards. */
 int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out);

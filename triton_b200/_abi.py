@@ -88,6 +88,8 @@ _SIGS = {
     "tri_batch_destroy": (C.c_int, [_vp]),
     "tri_batch_set_members": (C.c_int, [_vp, C.c_int32, C.POINTER(_vp)]),
     "tri_batch_advance": (C.c_int, [_vp, C.c_int32, C.POINTER(BatchProgress)]),
+    "tri_batch_launch": (C.c_int, [_vp, C.c_int32]),
+    "tri_batch_wait": (C.c_int, [_vp, C.POINTER(BatchProgress)]),
     "tri_batch_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_batch_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "tri_selftest_division": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),

@@ -50,6 +50,15 @@ class Batch:
         check(lib().tri_batch_advance(self._h, int(max_steps), C.byref(p)))
         return p
 
+    def launch(self, steps):
+        """Queues `steps` batched steps and returns at once (see wait)."""
+        check(lib().tri_batch_launch(self._h, int(steps)))
+
+    def wait(self):
+        p = _abi.BatchProgress()
+        check(lib().tri_batch_wait(self._h, C.byref(p)))
+        return p
+
     def autotune(self, trial_steps=10):
         t = _abi.Tuning()
         check(lib().tri_batch_autotune(self._h, int(trial_steps), C.byref(t)))

@@ -28,6 +28,8 @@ struct tri_batch {
   bool own_stream = false;
   std::vector<tri_domain*> members;
   void* d_mem = nullptr;
+  int32_t* d_tile_mem = nullptr;  // member of every flux tile
+  int32_t* d_wet_mem = nullptr;   // member of every wet-dry block
   BatchCtl* d_ctl = nullptr;
   BatchCtl* h_ctl = nullptr;  // pinned
   int32_t* h_seen = nullptr;  // pinned, one per chunk slot
@@ -41,6 +43,7 @@ struct tri_batch {
   int graph_steps = 0;
   double tuned_ms = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool launched = false;  // tri_batch_launch without its tri_batch_wait yet
 };
 
 namespace {
@@ -107,12 +110,24 @@ int build_table(tri_batch* b) {
   for (tri_domain* d : b->members) tab.push_back(member_dev<T>(d, b->rb, tiles, wet));
   b->ntiles = tiles;
   b->nwet = wet;
-  if (b->d_mem) cudaFree(b->d_mem);
-  b->d_mem = nullptr;
+  for (void** p : {&b->d_mem, (void**)&b->d_tile_mem, (void**)&b->d_wet_mem}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
   drop_graph(b);
   if (tab.empty()) return TRI_OK;
+  std::vector<int32_t> tm(tiles), wm(wet);
+  for (size_t m = 0; m < tab.size(); m++) {
+    std::fill(tm.begin() + tab[m].tile_begin, tm.begin() + tab[m].tile_end, (int32_t)m);
+    const uint32_t w1 = m + 1 < tab.size() ? tab[m + 1].wet_begin : wet;
+    std::fill(wm.begin() + tab[m].wet_begin, wm.begin() + w1, (int32_t)m);
+  }
   TRI_CUDA_TRY(cudaMalloc(&b->d_mem, tab.size() * sizeof(MemberDev<T>)));
   TRI_CUDA_TRY(cudaMemcpy(b->d_mem, tab.data(), tab.size() * sizeof(MemberDev<T>), cudaMemcpyHostToDevice));
+  TRI_CUDA_TRY(cudaMalloc(&b->d_tile_mem, std::max<size_t>(tm.size(), 1) * sizeof(int32_t)));
+  TRI_CUDA_TRY(cudaMemcpy(b->d_tile_mem, tm.data(), tm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  TRI_CUDA_TRY(cudaMalloc(&b->d_wet_mem, std::max<size_t>(wm.size(), 1) * sizeof(int32_t)));
+  TRI_CUDA_TRY(cudaMemcpy(b->d_wet_mem, wm.data(), wm.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   int sms = 148, dev = 0, per_sm = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   batch_flux_occupancy<T>(b->variant, &per_sm);
@@ -162,6 +177,8 @@ BatchArgs batch_args(tri_batch* b) {
   BatchArgs a{};
   a.mem = b->d_mem;
   a.nm = (int)b->members.size();
+  a.tile_member = b->d_tile_mem;
+  a.wet_member = b->d_wet_mem;
   a.ctl = b->d_ctl;
   a.ntiles = b->ntiles;
   a.nwet_blocks = b->nwet;
@@ -211,6 +228,9 @@ int launch_batch(tri_batch* b, int n) {
 
 // Prepares every member's clock for a batched advance (members at or past
 // their end stay halted for the whole call); counts the members that step.
+// Clocks go to the device on the batch stream, ahead of the batched launches;
+// a member without a valid CFL dt (new, or state uploaded) gets it first on
+// its own stream.
 int prepare_members(tri_batch* b, int* runnable) {
   *runnable = 0;
   for (tri_domain* d : b->members) {
@@ -220,17 +240,44 @@ int prepare_members(tri_batch* b, int* runnable) {
     m->events = 0;
     m->steps = 0;
     const bool need_dt = live && !d->dt_valid && !m->time_increment_fixed;
-    if (need_dt) m->dt_key[m->rd] = kDtKeyInf;
-    int rc = domain_push_clock(d);
-    if (rc != TRI_OK) return rc;
     if (need_dt) {
-      rc = domain_launch_dt(d);
+      m->dt_key[m->rd] = kDtKeyInf;
+      int rc = domain_push_clock(d);
+      if (rc == TRI_OK) rc = domain_launch_dt(d);
       if (rc != TRI_OK) return rc;
+      TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
       d->dt_valid = true;
+    } else {
+      TRI_CUDA_TRY(cudaMemcpyAsync(d->clk, d->mirror, sizeof(DevClock), cudaMemcpyHostToDevice, b->stream));
     }
     if (live) (*runnable)++;
   }
-  for (tri_domain* d : b->members) TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return TRI_OK;
+}
+
+// Reads every member's clock back (one stream synchronization) and sums the
+// progress of the advance.
+int pull_members(tri_batch* b, tri_batch_progress* p) {
+  memset(p, 0, sizeof(*p));
+  for (tri_domain* d : b->members)
+    TRI_CUDA_TRY(cudaMemcpyAsync(d->mirror, d->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, b->stream));
+  TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  int64_t updates = 0;
+  for (tri_domain* d : b->members) {
+    const DevClock* m = d->mirror;
+    p->steps = std::max(p->steps, m->steps);
+    if (m->events) p->members_with_events++;
+    if (!(m->simtime < m->sim_duration)) p->members_ended++;
+    updates += (int64_t)m->steps * (int64_t)(d->desc.rows - 2) * (int64_t)(d->desc.cols - 2);
+  }
+  p->cell_updates = updates;
+  return TRI_OK;
+}
+
+int reset_ctl(tri_batch* b) {
+  b->h_ctl->halted = 0;
+  b->h_ctl->tile_next = 0;
+  TRI_CUDA_TRY(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
   return TRI_OK;
 }
 
@@ -298,6 +345,8 @@ int tri_batch_destroy(tri_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
   if (b->d_mem) cudaFree(b->d_mem);
+  if (b->d_tile_mem) cudaFree(b->d_tile_mem);
+  if (b->d_wet_mem) cudaFree(b->d_wet_mem);
   if (b->d_ctl) cudaFree(b->d_ctl);
   if (b->h_ctl) cudaFreeHost(b->h_ctl);
   if (b->h_seen) cudaFreeHost(b->h_seen);
@@ -312,6 +361,7 @@ int tri_batch_destroy(tri_batch* b) {
 
 int tri_batch_set_members(tri_batch* b, int32_t nmembers, tri_domain* const* members) {
   TRI_CHECK_ARG(b && nmembers >= 0 && (nmembers == 0 || members), "null argument");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
   std::vector<tri_domain*> next;
   int rc = check_members(b->prec, nmembers, members, next);
   if (rc != TRI_OK) return rc;
@@ -324,15 +374,13 @@ int tri_batch_set_members(tri_batch* b, int32_t nmembers, tri_domain* const* mem
 
 int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* p) {
   TRI_CHECK_ARG(b && p, "null argument");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
   TRI_CHECK_ARG(max_steps >= 0, "max_steps must be >= 0");
-  memset(p, 0, sizeof(*p));
   int runnable = 0;
   int rc = prepare_members(b, &runnable);
   if (rc != TRI_OK) return rc;
   if (runnable > 0 && max_steps > 0) {
-    b->h_ctl->halted = 0;
-    b->h_ctl->tile_next = 0;
-    TRI_CUDA_TRY(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
+    if ((rc = reset_ctl(b)) != TRI_OK) return rc;
     // chunks of 8 batched steps, two in flight; stop once every runnable
     // member has raised an event
     int left = max_steps, k = 0;
@@ -351,23 +399,34 @@ int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* p) {
       }
       k++;
     }
-    TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
   }
-  int64_t updates = 0;
-  for (tri_domain* d : b->members) {
-    TRI_CUDA_TRY(cudaMemcpy(d->mirror, d->clk, sizeof(DevClock), cudaMemcpyDeviceToHost));
-    const DevClock* m = d->mirror;
-    p->steps = std::max(p->steps, m->steps);
-    if (m->events) p->members_with_events++;
-    if (!(m->simtime < m->sim_duration)) p->members_ended++;
-    updates += (int64_t)m->steps * (int64_t)(d->desc.rows - 2) * (int64_t)(d->desc.cols - 2);
+  return pull_members(b, p);
+}
+
+int tri_batch_launch(tri_batch* b, int32_t steps) {
+  TRI_CHECK_ARG(b, "null batch");
+  TRI_CHECK_ARG(steps >= 0, "steps must be >= 0");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
+  int runnable = 0;
+  int rc = prepare_members(b, &runnable);
+  if (rc != TRI_OK) return rc;
+  if (runnable > 0 && steps > 0) {
+    if ((rc = reset_ctl(b)) != TRI_OK) return rc;
+    if ((rc = launch_batch(b, steps)) != TRI_OK) return rc;
   }
-  p->cell_updates = updates;
+  b->launched = true;
   return TRI_OK;
+}
+
+int tri_batch_wait(tri_batch* b, tri_batch_progress* p) {
+  TRI_CHECK_ARG(b && p, "null argument");
+  b->launched = false;
+  return pull_members(b, p);
 }
 
 int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile) {
   TRI_CHECK_ARG(b, "null batch");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
   TRI_CHECK_ARG(variant >= 0 && variant < kFluxVariants, "variant %d outside [0,%d)", variant, kFluxVariants);
   TRI_CHECK_ARG(rows_per_tile >= 1, "rows_per_tile must be >= 1");
   TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
@@ -378,6 +437,7 @@ int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile) {
 
 int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out) {
   TRI_CHECK_ARG(b && out, "null argument");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
   TRI_CHECK_ARG(!b->members.empty(), "autotune needs at least one member");
   TRI_CHECK_ARG(trial_steps >= 1, "trial_steps must be >= 1");
   // snapshot every member: current state, max depth and clock
@@ -436,11 +496,8 @@ int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out) {
       }
       int runnable = 0;
       if (rc == TRI_OK) rc = prepare_members(b, &runnable);
-      if (rc == TRI_OK) {
-        b->h_ctl->halted = 0;
-        cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream);
-        rc = launch_batch(b, 2);  // warm-up, also builds the graph
-      }
+      if (rc == TRI_OK) rc = reset_ctl(b);
+      if (rc == TRI_OK) rc = launch_batch(b, 2);  // warm-up, also builds the graph
       cudaEventRecord(e0, b->stream);
       if (rc == TRI_OK) rc = launch_batch(b, trial_steps);
       cudaEventRecord(e1, b->stream);

@@ -57,14 +57,57 @@ __device__ __forceinline__ float div_by_rcp<float>(float a, float, float y) {
   return a * y;
 }
 
-// Order-preserving key of a non-negative double for an unsigned atomic min.
-// NaN maps to +inf so it is never the minimum (the reference's
-// "a < m ? a : m" fold never selects a NaN either).
-__device__ __forceinline__ unsigned long long dt_key(double v) {
-  return (v != v) ? 0x7FF0000000000000ull : (unsigned long long)__double_as_longlong(v);
+// a / b rounded to nearest for a divisor b shared by several quotients, from
+// y = RN(1/b): div_by_rcp where Markstein's conditions provably hold (|a| >=
+// 2^-900 so the residual a - b*q0 is exact, and q0 = RN(a*y) between 2^-1000
+// and 2^1000 so the quotient is normal), a plain division otherwise.  A zero
+// dividend gives the signed zero of a/b.  Bit-identical to a / b for every
+// finite non-zero b; the solver divides by Roe-averaged celerities, sums of
+// sqrt(h) and the friction term this way.
+__device__ __forceinline__ double div_shared(double a, double b, double y) {
+  const double q0 = a * y;
+  const unsigned long long ba = (unsigned long long)__double_as_longlong(a);
+  const unsigned long long ea = ba & 0x7FF0000000000000ull;
+  const unsigned long long eq = (unsigned long long)__double_as_longlong(q0) & 0x7FF0000000000000ull;
+  if ((ba << 1) != 0 && (ea < 0x07B0000000000000ull || eq < 0x0170000000000000ull || eq > 0x7E70000000000000ull))
+    return a / b;
+  const double r = fma(-q0, b, a);
+  return r == 0.0 ? q0 : fma(r, y, q0);
 }
-__device__ __forceinline__ unsigned long long dt_key(float v) { return dt_key((double)v); }
+// FP32 form: one multiplication (within 1.5 ulp).
+__device__ __forceinline__ float div_shared(float a, float, float y) { return a * y; }
 
+// The CFL dt of a wet cell is RN(A / D) with A = RN(courant*dx) and the wave
+// speed D = maxu + sqrt(g)*sqrt(h) (compute_dt_and_sqrt, kernels.h:167-193).
+// RN(A / D) never increases with D, so the minimum over cells of the dt is
+// RN(A / max D): the kernels reduce the largest D and divide once.  The slot
+// holds kDtKeyInf - bits(D), an order-reversing key (bits of a non-negative
+// double order like the double) under an unsigned atomic min; kDtKeyInf is
+// the empty slot (no wet cell), and NaN speeds are left out (the reference's
+// "a < m ? a : m" fold never selects a NaN dt).
 constexpr unsigned long long kDtKeyInf = 0x7FF0000000000000ull;
+__host__ __device__ inline unsigned long long speed_key(double d) {
+  if (!(d >= 0.0)) return kDtKeyInf;
+  unsigned long long b;
+#ifdef __CUDA_ARCH__
+  b = (unsigned long long)__double_as_longlong(d);
+#else
+  __builtin_memcpy(&b, &d, 8);
+#endif
+  return kDtKeyInf - (b > kDtKeyInf ? kDtKeyInf : b);
+}
+// dt of a slot: RN(A / D) for the largest speed, DBL_MAX for an empty slot.
+__host__ __device__ inline double dt_of_key(unsigned long long key, double cfl_a) {
+  if (key >= kDtKeyInf) return 1.7976931348623157e308;
+  const unsigned long long b = kDtKeyInf - key;
+  double d;
+#ifdef __CUDA_ARCH__
+  d = __longlong_as_double((long long)b);
+#else
+  __builtin_memcpy(&d, &b, 8);
+#endif
+  return cfl_a / d;
+}
+
 
 }  // namespace tri

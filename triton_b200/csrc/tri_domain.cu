@@ -408,6 +408,7 @@ int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out)
     return fail(set_error(TRI_E_CUDA, "clock allocation failed"));
   memset(d->mirror, 0, sizeof(DevClock));
   d->mirror->dt_key[0] = d->mirror->dt_key[1] = kDtKeyInf;
+  d->mirror->cfl_a = desc->courant * desc->cell_size;
   d->mirror->sim_duration = 0;
   d->mirror->print_interval = 1e300;
   d->mirror->print_observation = 1e300;
@@ -778,14 +779,7 @@ int tri_domain_compute_dt(tri_domain* d, double* local_dt) {
   rc = pull_clock(d);
   if (rc != TRI_OK) return rc;
   d->dt_valid = true;
-  const unsigned long long key = m->dt_key[m->rd];
-  double v;
-  if (key >= kDtKeyInf) {
-    v = 1.7976931348623157e308;
-  } else {
-    memcpy(&v, &key, 8);
-  }
-  *local_dt = v;
+  *local_dt = dt_of_key(m->dt_key[m->rd], m->cfl_a);
   return TRI_OK;
 }
 

@@ -33,8 +33,9 @@ __device__ __forceinline__ CellQ<T> make_cell(T h, T qx, T qy, T z, T hextra) {
   c.z = z;
   c.sq = dev_fmax(dev_sqrt(h), T(0));
   if (h >= hextra) {
-    c.u = qx / h;
-    c.v = qy / h;
+    const T rh = T(1) / h;
+    c.u = div_shared(qx, h, rh);
+    c.v = div_shared(qy, h, rh);
   } else {
     c.u = T(0);
     c.v = T(0);
@@ -76,8 +77,11 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   const T h12 = T(0.5) * (h1 + h2);
   const T dh = h2 - h1;
   const T c12 = dev_sqrt(G * h12);
-  const T u12 = (u1 * sqh1 + u2 * sqh2) / (sqh1 + sqh2);
-  const T v12 = (v1 * sqh1 + v2 * sqh2) / (sqh1 + sqh2);
+  const T rc12 = T(1) / c12;  // shared divisors: exact quotients via div_shared
+  const T ssq = sqh1 + sqh2;
+  const T rssq = T(1) / ssq;
+  const T u12 = div_shared(u1 * sqh1 + u2 * sqh2, ssq, rssq);
+  const T v12 = div_shared(v1 * sqh1 + v2 * sqh2, ssq, rssq);
   const T un = u12 * nx + v12 * ny;
   T lam0 = un - c12, lam1 = un, lam2 = un + c12;
   T lamE0 = T(0), lamE2 = T(0);  // lamE1 is always zero
@@ -105,9 +109,10 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
 
   // wave strengths
   const T dqx = c2.qx - c1.qx, dqy = c2.qy - c1.qy;
-  const T al0 = T(0.5) * (dh - ((dqx * nx + dqy * ny) - un * dh) / c12);
-  const T al1 = ((dqy - v12 * dh) * nx - (dqx - u12 * dh) * ny) / c12;
-  const T al2 = T(0.5) * (dh + ((dqx * nx + dqy * ny) - un * dh) / c12);
+  const T aq = div_shared((dqx * nx + dqy * ny) - un * dh, c12, rc12);
+  const T al0 = T(0.5) * (dh - aq);
+  const T al1 = div_shared((dqy - v12 * dh) * nx - (dqx - u12 * dh) * ny, c12, rc12);
+  const T al2 = T(0.5) * (dh + aq);
 
   // upwinded bed-step source, limited where the step is higher than the water
   const T z1 = c1.z, z2 = c2.z;
@@ -120,26 +125,27 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     hp = h2;
     if (z2 + h2 < z1) dzp = -h2;
   }
-  T be0 = T(0.5) * G * (hp - T(0.5) * dev_fabs(dzp)) * dzp / c12;
+  T be0 = div_shared(T(0.5) * G * (hp - T(0.5) * dev_fabs(dzp)) * dzp, c12, rc12);
 
   // positivity limiter on subcritical wet-wet faces
   hp = h1 + al0;
   if (lam0 * lam2 < T(0) && hp > T(0) && h1 > T(0) && h2 > T(0)) {
-    be0 = dev_fmax(be0, lam0 / (lam0 + lamE2) * (al0 * lam0 - div_by_rcp(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
-    be0 = dev_fmin(be0, lam2 / (lam2 + lamE0) * (-al2 * lam2 + div_by_rcp(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
+    // lam/(lam + lamE) is exactly 1 without an entropy-fix part (lam != 0 here)
+    const T f0 = lamE2 == T(0) ? T(1) : lam0 / (lam0 + lamE2);
+    const T f2 = lamE0 == T(0) ? T(1) : lam2 / (lam2 + lamE0);
+    be0 = dev_fmax(be0, f0 * (al0 * lam0 - div_by_rcp(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
+    be0 = dev_fmin(be0, f2 * (-al2 * lam2 + div_by_rcp(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
   }
   const T be2 = -be0;
   const T be1 = T(0);
 
-  // intermediate states decide whether mass is redirected from a dry side
-  const T l1 = hp - be0 / lam0;
-  const T l2 = hp + be2 / lam2;
-
+  // intermediate states decide whether mass is redirected from a dry side;
+  // they only matter next to a dry cell, so they are formed only there
   T p0 = T(0), p1 = T(0), p2 = T(0);  // owner side
   T q0 = T(0), q1 = T(0), q2 = T(0);  // neighbour side
-  if (l2 < -E12 && h2 < E12) {
+  if (h2 < E12 && hp + be2 / lam2 < -E12) {
     p0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
-  } else if (l1 < -E12 && h1 < E12) {
+  } else if (h1 < E12 && hp - be0 / lam0 < -E12) {
     q0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
   } else {
     // wave 0: eigenvector (1, r01, r02)

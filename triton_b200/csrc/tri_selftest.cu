@@ -1,7 +1,9 @@
 // tri_selftest.cu -- tri_selftest_division: checks on the device that the
-// exact quotient from a correctly rounded reciprocal (div_by_rcp) equals the
-// IEEE quotient bit for bit, over operands shaped like the step's
-// (dt*d/dx, h*dx/2/dt: magnitudes 1e-14 .. 1e7 over divisors 1e-3 .. 1e3).
+// exact quotients from a correctly rounded reciprocal equal the IEEE quotient
+// bit for bit: div_by_rcp over operands shaped like the step's (dt*d/dx,
+// h*dx/2/dt: magnitudes 1e-14 .. 1e7 over divisors 1e-3 .. 1e3) and
+// div_shared over every finite dividend magnitude (subnormals included,
+// zeros of both signs) and divisors of either sign from 1e-30 to 1e30.
 #include <cuda_runtime.h>
 
 #include "tri_common.cuh"
@@ -34,6 +36,14 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
     const double q = div_by_rcp(a, b, y);
     const double ref = a / b;
     if (__double_as_longlong(q) != __double_as_longlong(ref)) local++;
+    // div_shared over any finite dividend (subnormal to 1e300) and divisors
+    // 1e-30 .. 1e30
+    const unsigned long long r3 = mix(seed ^ (0x5DEECE66Dull + 2 * i)), r4 = mix(r3);
+    double a2 = exp10(-320.0 + 620.0 * unit(r3)) * ((r3 & 1) ? -1.0 : 1.0);
+    if ((r4 & 0x3F) == 0) a2 = (r4 & 0x40) ? -0.0 : 0.0;
+    const double b2 = exp10(-30.0 + 60.0 * unit(r4)) * ((r4 & 0x80) ? -1.0 : 1.0);
+    const double q2 = div_shared(a2, b2, 1.0 / b2);
+    if (__double_as_longlong(q2) != __double_as_longlong(a2 / b2)) local++;
   }
   if (local) atomicAdd(bad, local);
 }

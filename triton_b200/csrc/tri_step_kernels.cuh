@@ -43,8 +43,7 @@ __device__ __forceinline__ bool clock_step(DevClock* __restrict__ c) {
   double dt;
   if (!c->time_increment_fixed) {
     // compute_global_dt: dry fallback, then clamp to the next print time
-    const unsigned long long key = c->dt_key[c->rd];
-    dt = (key >= kDtKeyInf) ? 1.7976931348623157e308 : __longlong_as_double((long long)key);
+    dt = dt_of_key(c->dt_key[c->rd], c->cfl_a);
     if (dt >= kMaxValue - 1.0) dt = c->init_dt;
     const double tp = c->print_interval * (c->print_id + 1);
     if (t0 + dt > tp) dt = tp - t0;
@@ -155,8 +154,9 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     if (n2v > E12 && hn >= hextra && modM > E12) {
       const T tt = dt * G * n2v * modM / (hn * hn * dev_cbrt(hn));
       const T sq = dev_sqrt(T(1) + T(4) * tt);
-      qxij = T(-0.5) * (mx - mx * sq) / tt;
-      qyij = T(-0.5) * (my - my * sq) / tt;
+      const T rtt = T(1) / tt;
+      qxij = div_shared(T(-0.5) * (mx - mx * sq), tt, rtt);
+      qyij = div_shared(T(-0.5) * (my - my * sq), tt, rtt);
     } else {
       qxij = mx;
       qyij = my;
@@ -682,12 +682,19 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
       if (hij > mh0) maxh[id] = hij;
       if (arrival != nullptr && hij > arrival_depth && !(arrival[id] < 3.0e38f)) arrival[id] = simtime_now;
     }
-    if (incol && hij > hextra) {  // CFL dt in FP64 in both forms
-      const double hd = (double)hij;
-      const double sq = fmax(sqrt(hd), 0.0);
-      const double maxu = fmax(fabs((double)qxv), fabs((double)qyv)) / hd;
-      const double dtc = cn * dx / (maxu + kSqrtG * sq);
-      const unsigned long long k = dt_key(dtc);
+    if (incol && hij > hextra) {  // wave speed of the CFL dt (reduced as its maximum)
+      double d;
+      if (sizeof(T) == 8) {  // FP64: the reference's denominator, bit for bit
+        const double hd = (double)hij;
+        const double sq = fmax(sqrt(hd), 0.0);
+        const double maxu = fmax(fabs((double)qxv), fabs((double)qyv)) / hd;
+        d = maxu + kSqrtG * sq;
+      } else {  // FP32 form: speed in FP32, maximum and dt in FP64
+        const T sq = dev_fmax(dev_sqrt(hij), T(0));
+        const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
+        d = (double)(maxu + T(kSqrtG) * sq);
+      }
+      const unsigned long long k = speed_key(d);
       key = k < key ? k : key;
     }
     hm = h0;
@@ -739,20 +746,6 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
 // blocks are a concatenation of every member's bands.
 // ===========================================================================
 template <typename T>
-__device__ __forceinline__ int member_of(const MemberDev<T>* __restrict__ mem, int nm, uint32_t x, bool tiles) {
-  int lo = 0, hi = nm - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    const uint32_t b = tiles ? mem[mid].tile_begin : mem[mid].wet_begin;
-    if (b <= x)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
-
-template <typename T>
 __global__ void k_batch_clock(const MemberDev<T>* __restrict__ mem, int nm, BatchCtl* __restrict__ ctl) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) ctl->tile_next = 0;
@@ -760,7 +753,8 @@ __global__ void k_batch_clock(const MemberDev<T>* __restrict__ mem, int nm, Batc
 }
 
 template <typename T, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __restrict__ mem, int nm,
+__global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __restrict__ mem,
+                                                          const int32_t* __restrict__ tile_member,
                                                           BatchCtl* __restrict__ ctl, uint32_t ntiles) {
   const int lane = threadIdx.x & 31;
   while (true) {
@@ -768,8 +762,7 @@ __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __
     if (lane == 0) tile = atomicAdd(&ctl->tile_next, 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
-    const int m = member_of<T>(mem, nm, tile, true);
-    const MemberDev<T>& M = mem[m];
+    const MemberDev<T>& M = mem[tile_member[tile]];
     if (!M.clk->active) continue;
     const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
                                      M.hextra);
@@ -778,9 +771,9 @@ __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* __restrict__ mem, int nm) {
-  const int m = member_of<T>(mem, nm, blockIdx.x, false);
-  const MemberDev<T>& M = mem[m];
+__global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* __restrict__ mem,
+                                                            const int32_t* __restrict__ wet_member) {
+  const MemberDev<T>& M = mem[wet_member[blockIdx.x]];
   DevClock* clk = M.clk;
   if (!clk->active) return;
   const uint32_t local = blockIdx.x - M.wet_begin;

@@ -102,9 +102,9 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
   const MemberDev<T>* mem = (const MemberDev<T>*)a.mem;
   k_batch_clock<T><<<(a.nm + 127) / 128, 128, 0, s>>>(mem, a.nm, a.ctl);
   switch (a.flux_variant) {
-    case 0: k_batch_flux<T, 3><<<a.flux_blocks, 128, 0, s>>>(mem, a.nm, a.ctl, a.ntiles); break;
-    case 1: k_batch_flux<T, 4><<<a.flux_blocks, 128, 0, s>>>(mem, a.nm, a.ctl, a.ntiles); break;
-    default: k_batch_flux<T, 5><<<a.flux_blocks, 128, 0, s>>>(mem, a.nm, a.ctl, a.ntiles); break;
+    case 0: k_batch_flux<T, 3><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
+    case 1: k_batch_flux<T, 4><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
+    default: k_batch_flux<T, 5><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
   }
   for (int w = 0; w < a.n_src_waves; w++) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
@@ -114,7 +114,7 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
     const int off = a.bc_waves[w], cnt = a.bc_waves[w + 1] - off;
     k_batch_extbc<T><<<(cnt + 127) / 128, 128, 0, s>>>(mem, a.bc_items + off, cnt);
   }
-  k_batch_wetdry<T><<<a.nwet_blocks, kWetCols, 0, s>>>(mem, a.nm);
+  k_batch_wetdry<T><<<a.nwet_blocks, kWetCols, 0, s>>>(mem, a.wet_member);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;
 }

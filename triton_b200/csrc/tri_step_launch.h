@@ -64,6 +64,8 @@ void flux_occupancy(int variant, int* per_sm);
 struct BatchArgs {
   const void* mem;  // MemberDev<T>[nm] in device memory
   int nm;
+  const int32_t* tile_member;  // member of every flux tile
+  const int32_t* wet_member;   // member of every wet-dry block
   BatchCtl* ctl;
   uint32_t ntiles, nwet_blocks;
   int flux_blocks, flux_variant;

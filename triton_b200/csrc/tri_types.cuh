@@ -20,6 +20,7 @@ struct DevClock {
   double init_dt, time_step, average_dt, global_dt;
   double t_step;  // simtime at the start of the running step
   double rdt;     // RN(1/global_dt)
+  double cfl_a;   // RN(courant * dx): the CFL dt is cfl_a / (largest wave speed)
   int32_t print_id, it_count, it_print, time_series, time_increment_fixed;
   int32_t runoff_row, src_idx_low, src_idx_high;
   int32_t active, halt, events, steps;

@@ -202,16 +202,36 @@ def _value_noise(rng, n_rows, n_cols, octaves=8, hurst=0.8):
     return out
 
 
+def _value_noise_torch(seed, n_rows, n_cols, octaves=8, hurst=0.8):
+    """_value_noise drawn on the GPU with torch (same octave lattices and
+    bilinear interpolation, torch's generator): seconds become milliseconds
+    on 4096^2 grids.  Returns a float64 numpy array."""
+    import torch
+    import torch.nn.functional as F
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(seed))
+    out = torch.zeros((n_rows, n_cols), dtype=torch.float64, device="cuda")
+    for k in range(octaves):
+        cells = 2 ** (k + 1)
+        lat = torch.randn((1, 1, cells + 1, cells + 1), generator=g, device="cuda", dtype=torch.float64)
+        out += F.interpolate(lat, size=(n_rows, n_cols), mode="bilinear", align_corners=True)[0, 0] * \
+            2.0 ** (-hurst * k)
+    return out.cpu().numpy()
+
+
 def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, rain_hours=1.0,
               manning_median=0.035, manning_sigma=0.3, relief=300.0, valley_depth=40.0, peak_flow=500.0,
-              nsrc=3, print_interval=None):
+              nsrc=3, print_interval=None, gpu_noise=False):
     """Fractal watershed: value-noise DEM rescaled to 0..relief m with a carved
     meandering valley draining to the southern (lowest) edge, log-normal
     Manning, `nsrc` triangular inflow hydrographs (0 -> peak at 2 h -> 0 at
     4 h), uniform rain for `rain_hours`, and an open (extbc type 0) outflow
     along the southern edge."""
     rng = np.random.default_rng(seed)
-    dem = _value_noise(np.random.default_rng(rng.integers(1 << 31)), n, n)
+    if gpu_noise:  # same recipe, terrain and roughness drawn on the GPU
+        dem = _value_noise_torch(rng.integers(1 << 31), n, n)
+    else:
+        dem = _value_noise(np.random.default_rng(rng.integers(1 << 31)), n, n)
     dem = (dem - dem.min()) / max(dem.max() - dem.min(), 1e-12) * relief
     # tilt toward the south edge so it is the lowest
     rows = np.arange(n)[:, None]
@@ -223,8 +243,15 @@ def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, r
     dist = np.abs(cols - xc) / halfw
     carve = valley_depth * np.exp(-dist ** 2)
     dem = np.maximum(dem - carve, 0.0)
-    mann = np.exp(np.log(manning_median) + manning_sigma * np.random.default_rng(rng.integers(1 << 31))
-                  .standard_normal((n, n)))
+    if gpu_noise:
+        import torch
+        gm = torch.Generator(device="cuda")
+        gm.manual_seed(int(rng.integers(1 << 31)))
+        mann = torch.exp(np.log(manning_median) + manning_sigma * torch.randn(
+            (n, n), generator=gm, device="cuda", dtype=torch.float64)).cpu().numpy()
+    else:
+        mann = np.exp(np.log(manning_median) + manning_sigma * np.random.default_rng(rng.integers(1 << 31))
+                      .standard_normal((n, n)))
     z = _walls(dem)
     n2 = _copy_ghosts(_pad(mann)) ** 2
     zero = np.zeros_like(z)
