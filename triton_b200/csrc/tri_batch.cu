@@ -82,7 +82,7 @@ MemberDev<T> member_dev(tri_domain* d, int rb, uint32_t& tiles, uint32_t& wet) {
   m.tile_end = tiles;
   m.wet_nbx = (uint32_t)((a.cols + kWetCols - 1) / kWetCols);
   m.wet_begin = wet;
-  wet += m.wet_nbx * (uint32_t)((a.rows + kWetBand - 1) / kWetBand);
+  wet += m.wet_nbx * (uint32_t)((a.rows + kStageBand<T> - 1) / kStageBand<T>);
   m.nsrc = a.nsrc;
   m.src_cells = a.src_cells;
   m.hyg_t = a.hyg_t;
@@ -239,6 +239,7 @@ int prepare_members(tri_batch* b, int* runnable) {
     m->halt = live ? 0 : 1;
     m->events = 0;
     m->steps = 0;
+    m->status = 0;
     const bool need_dt = live && !d->dt_valid && !m->time_increment_fixed;
     if (need_dt) {
       m->dt_key[m->rd] = kDtKeyInf;
@@ -271,6 +272,10 @@ int pull_members(tri_batch* b, tri_batch_progress* p) {
     updates += (int64_t)m->steps * (int64_t)(d->desc.rows - 2) * (int64_t)(d->desc.cols - 2);
   }
   p->cell_updates = updates;
+  for (tri_domain* d : b->members)
+    if (d->mirror->status != 0)
+      return set_error(TRI_E_TIMEOUT, "a device-side wait gave up during the last batched advance (status %d)",
+                       d->mirror->status);
   return TRI_OK;
 }
 

@@ -98,7 +98,7 @@ int64_t footprint_bytes(const tri_grid_desc* g) {
   const int64_t n = (int64_t)g->rows * g->cols;
   const int64_t es = g->precision == TRI_FP32 ? 4 : 8;
   // 6 state buffers + z + n2 + maxh, one FP64 staging field, runoff zone ids
-  return n * es * 9 + n * 8 + n * 4 + (1 << 20);
+  return n * es * 9 + 9 * (int64_t)kFieldPad + n * 8 + n * 4 + (1 << 20);
 }
 
 template <typename T>
@@ -135,9 +135,9 @@ __global__ void k_observe(const DevClock* __restrict__ clk, StateBufs<T> sb, con
   if (k >= nobs) return;
   const int b = clk->cur;
   const int id = cells[k];
-  out[k] = (double)sb.h[b][id];
-  out[nobs + k] = (double)sb.qx[b][id];
-  out[2 * nobs + k] = (double)sb.qy[b][id];
+  out[k] = (double)sb.H(b)[id];
+  out[nobs + k] = (double)sb.QX(b)[id];
+  out[2 * nobs + k] = (double)sb.QY(b)[id];
 }
 
 // Interior volume: each block sums a fixed set of rows in a fixed order, then
@@ -145,7 +145,7 @@ __global__ void k_observe(const DevClock* __restrict__ clk, StateBufs<T> sb, con
 template <typename T>
 __global__ void __launch_bounds__(256) k_volume_part(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows,
                                                      int cols, double* __restrict__ part) {
-  const T* h = sb.h[clk->cur];
+  const T* h = sb.H(clk->cur);
   double acc = 0.0;
   for (int r = 1 + blockIdx.x; r <= rows - 2; r += gridDim.x)
     for (int c = 1 + threadIdx.x; c <= cols - 2; c += blockDim.x) acc += (double)h[(size_t)r * cols + c];
@@ -388,7 +388,7 @@ int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out)
   const size_t fb = d->ncells * d->esize;
   void** fields[] = {&d->h[0], &d->h[1], &d->qx[0], &d->qx[1], &d->qy[0], &d->qy[1], &d->z, &d->n2, &d->maxh};
   for (void** f : fields) {
-    cudaError_t e = cudaMalloc(f, fb);
+    cudaError_t e = cudaMalloc(f, fb + kFieldPad);
     if (e != cudaSuccess)
       return fail(set_error(e == cudaErrorMemoryAllocation ? TRI_E_NOMEM : TRI_E_CUDA, "cudaMalloc(%zu): %s", fb,
                             cudaGetErrorString(e)));
@@ -418,6 +418,8 @@ int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out)
       cudaMalloc((void**)&d->vol_out, sizeof(double)) != cudaSuccess)
     return fail(set_error(TRI_E_CUDA, "volume scratch allocation failed"));
   for (int i = 0; i < 2; i++) cudaEventCreateWithFlags(&d->chunk_ev[i], cudaEventDisableTiming);
+  rc = d->prec == TRI_FP64 ? prepare_kernels<double>() : prepare_kernels<float>();
+  if (rc != TRI_OK) return fail(rc);
   choose_shape(d);
   rc = push_clock(d);
   if (rc != TRI_OK) return fail(rc);
@@ -765,6 +767,9 @@ int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* p) {
   if (rc != TRI_OK) return rc;
   p->steps = m->steps;
   p->events = m->events;
+  if (m->status != 0)
+    return set_error(TRI_E_TIMEOUT, "a device-side wait gave up during the last advance (status %d); the state "
+                     "of this domain is not valid", m->status);
   return TRI_OK;
 }
 

@@ -7,4 +7,5 @@ template int launch_initial_dt<float>(const StepArgs&, cudaStream_t);
 template void flux_occupancy<float>(int, int*);
 template int launch_batch_step<float>(const BatchArgs&, cudaStream_t);
 template void batch_flux_occupancy<float>(int, int*);
+template int prepare_kernels<float>();
 }  // namespace tri

@@ -7,4 +7,5 @@ template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);
 template void flux_occupancy<double>(int, int*);
 template int launch_batch_step<double>(const BatchArgs&, cudaStream_t);
 template void batch_flux_occupancy<double>(int, int*);
+template int prepare_kernels<double>();
 }  // namespace tri

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "tri_common.cuh"
+#include "tri_bulk.cuh"
 #include "tri_face.cuh"
 #include "tri_step_launch.h"
 #include "tri_types.cuh"
@@ -204,12 +205,12 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   FluxCtx<T> X;
   X.clk = clk;
   const int src = clk->src, dst = clk->dst;
-  X.hi = sb.h[src];
-  X.qxi = sb.qx[src];
-  X.qyi = sb.qy[src];
-  X.ho = sb.h[dst];
-  X.qxo = sb.qx[dst];
-  X.qyo = sb.qy[dst];
+  X.hi = sb.H(src);
+  X.qxi = sb.QX(src);
+  X.qyi = sb.QY(src);
+  X.ho = sb.H(dst);
+  X.qxo = sb.QX(dst);
+  X.qyo = sb.QY(dst);
   X.bed = bed;
   X.n2 = n2;
   X.zone = zone;
@@ -397,7 +398,7 @@ __global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int
   const int lo = clk->src_idx_low, hi = clk->src_idx_high;
   const T dt = T(clk->global_dt);
   const T simtime = T(clk->t_step);
-  T* h = sb.h[clk->dst];
+  T* h = sb.H(clk->dst);
   const T flo = hyg_v[(size_t)lo * nsrc + id];
   const T fhi = hyg_v[(size_t)hi * nsrc + id];
   const T tlo = T(hyg_t[lo]), thi = T(hyg_t[hi]);
@@ -421,9 +422,9 @@ template <typename T>
 __global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows, int cols) {
   if (!clk->active) return;
   const int d = clk->dst;
-  T* h = sb.h[d];
-  T* qx = sb.qx[d];
-  T* qy = sb.qy[d];
+  T* h = sb.H(d);
+  T* qx = sb.QX(d);
+  T* qy = sb.QY(d);
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   // Final values of copy_info_to_exterior_boundaries_west_east followed by
   // _north_south: ghost columns take the adjacent interior column (rows
@@ -457,9 +458,9 @@ __device__ __forceinline__ void extbc_apply(DevClock* __restrict__ clk, const St
                                             const int32_t* __restrict__ nrowsv, const T* __restrict__ var1,
                                             const T* __restrict__ var2, int rows, int cols) {
   const int d = clk->dst;
-  T* h = sb.h[d];
-  T* qx = sb.qx[d];
-  T* qy = sb.qy[d];
+  T* h = sb.H(d);
+  T* qx = sb.QX(d);
+  T* qy = sb.QY(d);
   const T dt = T(clk->global_dt);
   const T simtime = T(clk->t_step);
   const int ii = cells[id];
@@ -617,9 +618,9 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
                                                           float* __restrict__ arrival, float arrival_depth, int bx,
                                                           int by) {
   const int buf = WETDRY ? clk->dst : clk->cur;
-  const T* __restrict__ h = sb.h[buf];
-  T* __restrict__ qx = sb.qx[buf];
-  T* __restrict__ qy = sb.qy[buf];
+  const T* __restrict__ h = sb.H(buf);
+  T* __restrict__ qx = sb.QX(buf);
+  T* __restrict__ qy = sb.QY(buf);
   const T E12 = eps12<T>();
   const int lane = threadIdx.x & 31;
   const int c = bx * kWetCols + threadIdx.x;
@@ -708,6 +709,160 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
   return key;
 }
 
+// ---------------------------------------------------------------------------
+// Staged wet-dry/dt: one block per band of WetStage<T>::kBand rows x
+// kWetCols columns.  The block first stages, in shared memory, its rows of h
+// and the bed with a halo row above and below, and its rows of qx, qy and the
+// maximum depth, each row from column c0-1 to c0+kWetCols (clipped to the
+// grid) with one bulk asynchronous copy (cp.async.bulk: rounded out to
+// 16-byte boundaries, which every field's kFieldPad allows at its end), all
+// completing on one mbarrier, so a block has its whole tile in flight at
+// once.  The FP32 form then turns the staged bed offsets into levels relative
+// to one reference in place (one conversion per staged cell).  Then each
+// thread walks one column down the band from shared memory.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct WetStage {
+  static constexpr int kBand = kStageBand<T>;                        // rows per block
+  static constexpr int kVec = 16 / (int)sizeof(T);                   // elements per 16 bytes
+  static constexpr int kCap = kWetCols + 2 + 2 * (kVec - 1);         // elements per row buffer
+  static constexpr int kHRows = kBand + 2;                           // h and bed rows (with halos)
+  static constexpr int kRows = 2 * kHRows + 3 * kBand;               // + qx, qy, max depth rows
+  static constexpr size_t kData = (size_t)kRows * kCap * sizeof(T);
+  static constexpr size_t kBytes = kData + 16 + 4 * kHRows;          // + mbarrier + row offsets
+};
+
+template <typename T>
+__device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict__ clk, const StateBufs<T>& sb,
+                                                            const BedMap<T>& bed, T* __restrict__ maxh, int rows,
+                                                            int cols, T hextra, float* __restrict__ arrival,
+                                                            float arrival_depth, int bx, int by, T* stage) {
+  using S = WetStage<T>;
+  const int buf = clk->dst;
+  T* __restrict__ qx = sb.QX(buf);
+  T* __restrict__ qy = sb.QY(buf);
+  const T E12 = eps12<T>();
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int c0 = bx * kWetCols;
+  const int ra = by * S::kBand;
+  const int rz = min(ra + S::kBand - 1, rows - 1);
+  const int cl = max(c0 - 1, 0), ce = min(c0 + kWetCols + 1, cols);  // staged columns [cl, ce)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(stage) + S::kData);
+  // offs[j]: column c of staged row ra-1+j sits at buffer index c + offs[j]
+  int* offs = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(stage) + S::kData + 16);
+  if (tid == 0) mbar_init(bar, 1);
+  if (tid < S::kHRows) {
+    const int64_t r = (int64_t)(ra - 1 + tid);
+    offs[tid] = (int)(r * cols - ((r * cols + cl) & ~(int64_t)(S::kVec - 1)));
+  }
+  __syncthreads();
+  if (tid < 32) {
+    for (int k = lane; k < S::kRows; k += 32) {
+      const T* src;
+      int r;
+      if (k < 2 * S::kHRows) {
+        r = ra - 1 + (k < S::kHRows ? k : k - S::kHRows);
+        src = k < S::kHRows ? (const T*)sb.H(buf) : (const T*)bed.z;
+        if (r < 0 || r > rows - 1) continue;
+      } else {
+        const int q = k - 2 * S::kHRows, f = q / S::kBand;
+        r = ra + (q - f * S::kBand);
+        src = f == 0 ? (const T*)qx : (f == 1 ? (const T*)qy : (const T*)maxh);
+        if (r > rz) continue;
+      }
+      const int64_t e0 = ((int64_t)r * cols + cl) & ~(int64_t)(S::kVec - 1);
+      const int64_t e1 = ((int64_t)r * cols + ce + S::kVec - 1) & ~(int64_t)(S::kVec - 1);
+      const uint32_t bytes = (uint32_t)((e1 - e0) * (int64_t)sizeof(T));
+      mbar_expect_tx(bar, bytes);
+      bulk_g2s(stage + (size_t)k * S::kCap, src + e0, bytes, bar);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(bar);
+  }
+  if (!mbar_wait(bar, 0)) {
+    // a copy never completed: report it, wait (bounded) once more so no copy
+    // still writes this block's shared memory when it exits, contribute nothing
+    atomicExch(&clk->status, kStatusStageTimeout);
+    mbar_wait(bar, 0);
+    return kDtKeyInf;
+  }
+  T* sh = stage;
+  T* sz = stage + (size_t)S::kHRows * S::kCap;
+  const T* sqx = stage + (size_t)2 * S::kHRows * S::kCap;
+  const T* sqy = sqx + (size_t)S::kBand * S::kCap;
+  const T* smh = sqy + (size_t)S::kBand * S::kCap;
+  const double zref = bed.ref_of(ra, min(c0, cols - 1));
+  if (sizeof(T) == 4) {  // bed offsets -> levels relative to zref, in place
+    const int w = ce - cl;
+    for (int e = tid; e < S::kHRows * w; e += kWetCols) {
+      const int j = e / w, c = cl + (e - j * w), r = ra - 1 + j;
+      if (r < 0 || r > rows - 1) continue;
+      T& zv = sz[(size_t)j * S::kCap + c + offs[j]];
+      zv = (T)bed.local_v(zv, r, c, zref);
+    }
+    __syncthreads();
+  }
+  const int c = c0 + tid;
+  const bool incol = c < cols;
+  const bool intcol = c >= 1 && c <= cols - 2;
+  const float simtime_now = (float)clk->simtime;
+  unsigned long long key = kDtKeyInf;
+  if (incol) {
+    int om = offs[0], o = offs[1];
+#pragma unroll
+    for (int jq = 0; jq < S::kBand; ++jq) {
+      const int r = ra + jq;
+      if (r > rz) break;
+      const int j = jq + 1;
+      const int op = offs[j + 1];
+      const size_t id = (size_t)r * cols + c;
+      const T* hrow = sh + (size_t)j * S::kCap + o;
+      const T hij = hrow[c];
+      T qxv = sqx[(size_t)jq * S::kCap + c + o], qyv = sqy[(size_t)jq * S::kCap + c + o];
+      if (intcol && r >= 1 && r <= rows - 2) {
+        const T* zrow = sz + (size_t)j * S::kCap + o;
+        const T zij = zrow[c];
+        if (hij > hextra) {
+          const T he = hrow[c + 1], hw = hrow[c - 1];
+          const T hm = sh[(size_t)(j - 1) * S::kCap + c + om];
+          const T hp = sh[(size_t)(j + 1) * S::kCap + c + op];
+          const T ze = zrow[c + 1], zw = zrow[c - 1];
+          const T zm = sz[(size_t)(j - 1) * S::kCap + c + om];
+          const T zp = sz[(size_t)(j + 1) * S::kCap + c + op];
+          if ((hij + zij < ze && he < E12) || (hij + zij < zw && hw < E12)) {
+            qxv = T(0);
+            qx[id] = T(0);
+          }
+          if ((hij + zij < zm && hm < E12) || (hij + zij < zp && hp < E12)) {
+            qyv = T(0);
+            qy[id] = T(0);
+          }
+        }
+        if (hij > smh[(size_t)jq * S::kCap + c + o]) maxh[id] = hij;
+        if (arrival != nullptr && hij > arrival_depth && !(arrival[id] < 3.0e38f)) arrival[id] = simtime_now;
+      }
+      if (hij > hextra) {  // wave speed of the CFL dt (reduced as its maximum)
+        double d;
+        if (sizeof(T) == 8) {  // FP64: the reference's denominator, bit for bit
+          const double hd = (double)hij;
+          const double sq = fmax(sqrt(hd), 0.0);
+          const double maxu = fmax(fabs((double)qxv), fabs((double)qyv)) / hd;
+          d = maxu + kSqrtG * sq;
+        } else {  // FP32 form: speed in FP32, maximum and dt in FP64
+          const T sq = dev_fmax(dev_sqrt(hij), T(0));
+          const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
+          d = (double)(maxu + T(kSqrtG) * sq);
+        }
+        const unsigned long long k = speed_key(d);
+        key = k < key ? k : key;
+      }
+      om = o;
+      o = op;
+    }
+  }
+  return key;
+}
+
 // Block minimum of the threads' keys, folded into *slot with one atomic.
 __device__ __forceinline__ void block_min_into(unsigned long long key, unsigned long long* slot) {
 #pragma unroll
@@ -722,7 +877,8 @@ __device__ __forceinline__ void block_min_into(unsigned long long key, unsigned 
   if (threadIdx.x == 0) {
     key = s_min[0];
     for (int w = 1; w < kWetCols / 32; w++) key = s_min[w] < key ? s_min[w] : key;
-    if (key < kDtKeyInf) atomicMin(slot, key);
+    // most blocks cannot lower the slot: read it first, then one atomic
+    if (key < kDtKeyInf && key < *reinterpret_cast<volatile unsigned long long*>(slot)) atomicMin(slot, key);
   }
 }
 
@@ -736,6 +892,19 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
   const unsigned long long key = wetdry_band<T, WETDRY>(clk, sb, bed, maxh, rows, cols, band, dx, cn, hextra,
                                                         arrival, arrival_depth, blockIdx.x, blockIdx.y);
   block_min_into(key, &clk->dt_key[WETDRY ? clk->wr : clk->rd]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict__ clk, StateBufs<T> sb,
+                                                            const BedMap<T> bed, T* __restrict__ maxh, int rows,
+                                                            int cols, T hextra, float* __restrict__ arrival,
+                                                            float arrival_depth) {
+  extern __shared__ __align__(128) unsigned char wet_smem[];
+  if (!clk->active) return;
+  if (sizeof(T) == 4 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  const unsigned long long key = wetdry_staged<T>(clk, sb, bed, maxh, rows, cols, hextra, arrival, arrival_depth,
+                                                  blockIdx.x, blockIdx.y, reinterpret_cast<T*>(wet_smem));
+  block_min_into(key, &clk->dt_key[clk->wr]);
 }
 
 // ===========================================================================
@@ -773,14 +942,15 @@ __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __
 template <typename T>
 __global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* __restrict__ mem,
                                                             const int32_t* __restrict__ wet_member) {
+  extern __shared__ __align__(128) unsigned char wet_smem[];
   const MemberDev<T>& M = mem[wet_member[blockIdx.x]];
   DevClock* clk = M.clk;
   if (!clk->active) return;
   const uint32_t local = blockIdx.x - M.wet_begin;
   if (sizeof(T) == 4 && local == 0 && threadIdx.x == 0) fold_accounts(clk);
   const unsigned long long key =
-      wetdry_band<T, true>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, kWetBand, M.dxd, M.courant, M.hextra, M.arrival,
-                           M.arrival_depth, (int)(local % M.wet_nbx), (int)(local / M.wet_nbx));
+      wetdry_staged<T>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, M.hextra, M.arrival, M.arrival_depth,
+                       (int)(local % M.wet_nbx), (int)(local / M.wet_nbx), reinterpret_cast<T*>(wet_smem));
   block_min_into(key, &clk->dt_key[clk->wr]);
 }
 
@@ -796,7 +966,7 @@ __global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2
   if (!clk->active) return;
   const int lo = clk->src_idx_low, hi = clk->src_idx_high;
   const T dt = T(clk->global_dt), simtime = T(clk->t_step);
-  T* h = M.sb.h[clk->dst];
+  T* h = M.sb.H(clk->dst);
   const T flo = M.hyg_v[(size_t)lo * M.nsrc + id], fhi = M.hyg_v[(size_t)hi * M.nsrc + id];
   const T tlo = T(M.hyg_t[lo]), thi = T(M.hyg_t[hi]);
   T flow;

@@ -70,10 +70,10 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
                                                  a.bc_types, a.bc_start, a.bc_nrows, (const T*)a.bc_v1,
                                                  (const T*)a.bc_v2, rows, cols);
   }
-  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + kWetBand - 1) / kWetBand);
+  dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + WetStage<T>::kBand - 1) / WetStage<T>::kBand);
   if (ev) cudaEventRecord(ev[2], s);
-  k_wetdry_dt<T, true><<<g2, kWetCols, 0, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, kWetBand, a.dx, a.courant, hx,
-                                               a.arrival, a.arrival_depth);
+  k_wetdry_staged<T><<<g2, kWetCols, WetStage<T>::kBytes, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, hx,
+                                                                 a.arrival, a.arrival_depth);
   if (ev) cudaEventRecord(ev[3], s);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;
@@ -114,8 +114,17 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
     const int off = a.bc_waves[w], cnt = a.bc_waves[w + 1] - off;
     k_batch_extbc<T><<<(cnt + 127) / 128, 128, 0, s>>>(mem, a.bc_items + off, cnt);
   }
-  k_batch_wetdry<T><<<a.nwet_blocks, kWetCols, 0, s>>>(mem, a.wet_member);
+  k_batch_wetdry<T><<<a.nwet_blocks, kWetCols, WetStage<T>::kBytes, s>>>(mem, a.wet_member);
   TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
+template <typename T>
+int prepare_kernels() {
+  TRI_CUDA_TRY(cudaFuncSetAttribute(k_wetdry_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)WetStage<T>::kBytes));
+  TRI_CUDA_TRY(cudaFuncSetAttribute(k_batch_wetdry<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)WetStage<T>::kBytes));
   return TRI_OK;
 }
 

@@ -15,7 +15,10 @@ namespace tri {
 constexpr int kStripCols = 30;   // interior columns per warp tile of the flux kernel
 constexpr int kFluxVariants = 3; // register budgets: >= 3, 4, 5 blocks of 128 threads per SM
 constexpr int kWetCols = 128;    // columns per block of the wet-dry/dt kernel
-constexpr int kWetBand = 16;     // rows per block of the wet-dry/dt kernel
+constexpr int kWetBand = 16;     // rows per block of the initial-dt kernel
+// rows per block of the staged wet-dry/dt kernel (its shared-memory tile)
+template <typename T>
+constexpr int kStageBand = sizeof(T) == 8 ? 4 : 8;
 
 struct StepArgs {
   DevClock* clk;
@@ -81,6 +84,13 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s);
 template <typename T>
 void batch_flux_occupancy(int variant, int* per_sm);
 
+// Kernel attributes (shared-memory sizes) on the current device; call before
+// the first launch on a device.
+template <typename T>
+int prepare_kernels();
+
+extern template int prepare_kernels<double>();
+extern template int prepare_kernels<float>();
 extern template int launch_step<double>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 extern template int launch_step<float>(const StepArgs&, cudaStream_t, cudaEvent_t*);
 extern template int launch_initial_dt<double>(const StepArgs&, cudaStream_t);

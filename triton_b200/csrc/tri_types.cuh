@@ -8,6 +8,10 @@
 
 namespace tri {
 
+// Every field allocation has this many bytes past its last element: bulk row
+// copies round their end up to a 16-byte boundary and may read into it.
+constexpr size_t kFieldPad = 256;
+
 // Volume accounting terms of the FP32 form: inflow through boundary faces,
 // point sources, runoff, external-boundary depth resets, negative-depth clipping.
 constexpr int kAccTerms = 5;
@@ -45,6 +49,11 @@ struct StateBufs {
   T* h[2];
   T* qx[2];
   T* qy[2];
+  // buffer i (0 or 1) by selection: indexing a kernel parameter's array with a
+  // runtime index would copy the whole struct to local memory
+  __device__ __forceinline__ T* H(int i) const { return i ? h[1] : h[0]; }
+  __device__ __forceinline__ T* QX(int i) const { return i ? qx[1] : qx[0]; }
+  __device__ __forceinline__ T* QY(int i) const { return i ? qy[1] : qy[0]; }
 };
 
 // The bed.  FP64 form: the DEM itself.  FP32 form: per 32x32 tile an FP64
@@ -61,6 +70,7 @@ struct BedMap<double> {
   int ntc;
   __device__ __forceinline__ double ref_of(int, int) const { return 0.0; }
   __device__ __forceinline__ double local(size_t id, int, int, double) const { return z[id]; }
+  __device__ __forceinline__ double local_v(double zv, int, int, double) const { return zv; }
   __device__ __forceinline__ double absolute(size_t id, int, int) const { return z[id]; }
 };
 template <>
@@ -72,6 +82,11 @@ struct BedMap<float> {
   __device__ __forceinline__ float local(size_t id, int r, int c, double ref) const {
     const double b = base[(r >> 5) * ntc + (c >> 5)];
     return b == ref ? z[id] : z[id] + (float)(b - ref);
+  }
+  // the same for an offset already read (from shared memory)
+  __device__ __forceinline__ float local_v(float zv, int r, int c, double ref) const {
+    const double b = base[(r >> 5) * ntc + (c >> 5)];
+    return b == ref ? zv : zv + (float)(b - ref);
   }
   __device__ __forceinline__ double absolute(size_t id, int r, int c) const {
     return base[(r >> 5) * ntc + (c >> 5)] + (double)z[id];
