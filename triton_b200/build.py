@@ -25,9 +25,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # reference's CPU build computes them; double division and sqrt are IEEE.
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
                   "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-# The FP32 precision form is held to a tolerance, not to bit parity: its unit
-# may contract products into FMAs and use the fast division and square root.
-PER_FILE = {"tri_step_f32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
+# The FP32 precision form is held to a tolerance against FP64, not to bit
+# parity; its approximate divisions are explicit intrinsics in the source.  No
+# compiler licence to contract products or approximate divisions: where a
+# compiler uses it depends on what a function was inlined into, and a member of
+# a batch must compute exactly what the same domain computes alone.
+PER_FILE = {"tri_step_f32.cu": ["--fmad=false", "-ftz=true"]}
 
 
 def _nvcc():

@@ -24,7 +24,13 @@ template <>
 __host__ __device__ constexpr float eps12<float>() { return 1e-12f; }
 
 __device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
+// FP32 form: the approximate hardware square root, one PTX instruction, so it
+// is the same in every kernel the solver is inlined into.
+__device__ __forceinline__ float dev_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 __device__ __forceinline__ double dev_cbrt(double x) { return cbrt(x); }
 __device__ __forceinline__ float dev_cbrt(float x) { return cbrtf(x); }
 __device__ __forceinline__ double dev_fabs(double x) { return fabs(x); }
@@ -76,6 +82,18 @@ __device__ __forceinline__ double div_shared(double a, double b, double y) {
 }
 // FP32 form: one multiplication (within 1.5 ulp).
 __device__ __forceinline__ float div_shared(float a, float, float y) { return a * y; }
+
+// Reciprocal of a divisor shared by several quotients.  FP64: RN(1/b), as
+// div_shared requires.  FP32 form: the hardware's approximate reciprocal
+// (within 2 ulp), written as an intrinsic so it is the same instruction in
+// every kernel the solver is inlined into (a compiler allowed to approximate
+// divisions may rewrite them differently in different contexts, and a batch
+// member must compute exactly what the same domain computes alone).
+__device__ __forceinline__ double recip(double b) { return 1.0 / b; }
+__device__ __forceinline__ float recip(float b) { return __fdividef(1.0f, b); }
+// a / b where the FP32 form accepts the approximate quotient (same reason).
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
 // The CFL dt of a wet cell is RN(A / D) with A = RN(courant*dx) and the wave
 // speed D = maxu + sqrt(g)*sqrt(h) (compute_dt_and_sqrt, kernels.h:167-193).

@@ -33,7 +33,7 @@ __device__ __forceinline__ CellQ<T> make_cell(T h, T qx, T qy, T z, T hextra) {
   c.z = z;
   c.sq = dev_fmax(dev_sqrt(h), T(0));
   if (h >= hextra) {
-    const T rh = T(1) / h;
+    const T rh = recip(h);
     c.u = div_shared(qx, h, rh);
     c.v = div_shared(qy, h, rh);
   } else {
@@ -77,9 +77,9 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   const T h12 = T(0.5) * (h1 + h2);
   const T dh = h2 - h1;
   const T c12 = dev_sqrt(G * h12);
-  const T rc12 = T(1) / c12;  // shared divisors: exact quotients via div_shared
+  const T rc12 = recip(c12);  // shared divisors: exact quotients via div_shared
   const T ssq = sqh1 + sqh2;
-  const T rssq = T(1) / ssq;
+  const T rssq = recip(ssq);
   const T u12 = div_shared(u1 * sqh1 + u2 * sqh2, ssq, rssq);
   const T v12 = div_shared(v1 * sqh1 + v2 * sqh2, ssq, rssq);
   const T un = u12 * nx + v12 * ny;

@@ -153,9 +153,9 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     const T my = c.qy - ry0 - ry1;
     const T modM = dev_sqrt(mx * mx + my * my);
     if (n2v > E12 && hn >= hextra && modM > E12) {
-      const T tt = dt * G * n2v * modM / (hn * hn * dev_cbrt(hn));
+      const T tt = fdiv(dt * G * n2v * modM, hn * hn * dev_cbrt(hn));
       const T sq = dev_sqrt(T(1) + T(4) * tt);
-      const T rtt = T(1) / tt;
+      const T rtt = recip(tt);
       qxij = div_shared(T(-0.5) * (mx - mx * sq), tt, rtt);
       qyij = div_shared(T(-0.5) * (my - my * sq), tt, rtt);
     } else {
@@ -692,7 +692,7 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
         d = maxu + kSqrtG * sq;
       } else {  // FP32 form: speed in FP32, maximum and dt in FP64
         const T sq = dev_fmax(dev_sqrt(hij), T(0));
-        const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
+        const T maxu = fdiv(dev_fmax(dev_fabs(qxv), dev_fabs(qyv)), hij);
         d = (double)(maxu + T(kSqrtG) * sq);
       }
       const unsigned long long k = speed_key(d);
@@ -850,7 +850,7 @@ __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict
           d = maxu + kSqrtG * sq;
         } else {  // FP32 form: speed in FP32, maximum and dt in FP64
           const T sq = dev_fmax(dev_sqrt(hij), T(0));
-          const T maxu = dev_fmax(dev_fabs(qxv), dev_fabs(qyv)) / hij;
+          const T maxu = fdiv(dev_fmax(dev_fabs(qxv), dev_fabs(qyv)), hij);
           d = (double)(maxu + T(kSqrtG) * sq);
         }
         const unsigned long long k = speed_key(d);

@@ -33,9 +33,9 @@ StateBufs<T> bufs_of(const StepArgs& a) {
 template <typename T>
 void flux_occupancy(int variant, int* per_sm) {
   switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 3>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 4>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, 5>, 128, 0); break;
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v0>, 128, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v1>, 128, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v2>, 128, 0); break;
   }
 }
 
@@ -49,9 +49,9 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], s);
 #define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx
   switch (a.flux_variant) {
-    case 0: k_flux_update<T, 3><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-    case 1: k_flux_update<T, 4><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-    default: k_flux_update<T, 5><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    case 0: k_flux_update<T, FluxBudget<T>::v0><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    case 1: k_flux_update<T, FluxBudget<T>::v1><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    default: k_flux_update<T, FluxBudget<T>::v2><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
   }
 #undef TRI_FLUX_ARGS
   if (ev) cudaEventRecord(ev[1], s);
@@ -91,9 +91,9 @@ int launch_initial_dt(const StepArgs& a, cudaStream_t s) {
 template <typename T>
 void batch_flux_occupancy(int variant, int* per_sm) {
   switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, 3>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, 4>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, 5>, 128, 0); break;
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v0>, 128, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v1>, 128, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v2>, 128, 0); break;
   }
 }
 
@@ -102,9 +102,9 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
   const MemberDev<T>* mem = (const MemberDev<T>*)a.mem;
   k_batch_clock<T><<<(a.nm + 127) / 128, 128, 0, s>>>(mem, a.nm, a.ctl);
   switch (a.flux_variant) {
-    case 0: k_batch_flux<T, 3><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
-    case 1: k_batch_flux<T, 4><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
-    default: k_batch_flux<T, 5><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
+    case 0: k_batch_flux<T, FluxBudget<T>::v0><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
+    case 1: k_batch_flux<T, FluxBudget<T>::v1><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
+    default: k_batch_flux<T, FluxBudget<T>::v2><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
   }
   for (int w = 0; w < a.n_src_waves; w++) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;

@@ -16,6 +16,19 @@ constexpr int kStripCols = 30;   // interior columns per warp tile of the flux k
 constexpr int kFluxVariants = 3; // register budgets: >= 3, 4, 5 blocks of 128 threads per SM
 constexpr int kWetCols = 128;    // columns per block of the wet-dry/dt kernel
 constexpr int kWetBand = 16;     // rows per block of the initial-dt kernel
+// Blocks per SM that the flux kernel's three register-budget variants are
+// compiled for (__launch_bounds__ minimum): FP64 needs about 128-150
+// registers a thread, the FP32 form 64-100.
+template <typename T>
+struct FluxBudget;
+template <>
+struct FluxBudget<double> {
+  static constexpr int v0 = 3, v1 = 4, v2 = 5;
+};
+template <>
+struct FluxBudget<float> {
+  static constexpr int v0 = 5, v1 = 6, v2 = 8;
+};
 // rows per block of the staged wet-dry/dt kernel (its shared-memory tile)
 template <typename T>
 constexpr int kStageBand = sizeof(T) == 8 ? 4 : 8;
