@@ -185,6 +185,107 @@ def reference_arm(args, sc, desc):
     print(json.dumps(line))
 
 
+def _timed(stream, fn):
+    """Runs fn() between two CUDA events on `stream`; returns (result, ms)."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def measure_forms(args, sc, stream, value64):
+    """The other forms on one GPU, after the headline measurement.
+
+    fp32: the same Thacker workload in the FP32 precision form.
+    ensemble: `--ens-members` watershed members (side log-uniform in
+    256..`--ens-max-side`, dx 5-20 m, rain 10-100 mm/h for 1 h, Manning
+    median +/-30 %, 3 h), advanced as one batch in FP32 and in FP64, and the
+    same members advanced one after another as plain FP64 domains; every
+    figure is interior cells x steps over CUDA-event time on one stream."""
+    from triton_b200 import scenarios
+    from triton_b200.batch import Batch
+    out = {}
+    d = sc.to_domain("fp32", stream=stream.cuda_stream)
+    d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    tune32 = d.autotune(trial_steps=8)
+    d.advance(args.warmup)
+    (n, _), ms = _timed(stream, lambda: d.advance(args.steps))
+    d.close()
+    v32 = sc.interior_cells * n / (ms / 1000.0)
+    out["fp32"] = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms / n, "vs_fp64": v32 / value64,
+                   "flux_launch_shape": {k: tune32[k] for k in ("variant", "rows_per_tile")}}
+    if args.ens_members <= 0:
+        return out
+    members = scenarios.ensemble(members=args.ens_members, seed=2024, side_min=256, side_max=args.ens_max_side,
+                                 duration=3 * 3600.0, gpu_noise=True)
+    cells = sum(m.interior_cells for m in members)
+    ens = {"members": len(members), "interior_cells": cells, "batched_steps": args.ens_steps,
+           "workload": f"{len(members)} rain-on-grid watersheds, side log-uniform 256..{args.ens_max_side}, "
+                       "dx 5-20 m, rain 10-100 mm/h for 1 h, Manning median +/-30 %, 3 h"}
+    for prec in ("fp32", "fp64"):
+        doms = [m.to_domain(prec, stream=stream.cuda_stream) for m in members]
+        for dm in doms:
+            dm.set_clock(print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+        b = Batch(doms, stream=stream.cuda_stream)
+        tune = b.autotune(3)
+        b.advance(args.warmup)
+        p, ms = _timed(stream, lambda: b.advance(args.ens_steps))
+        ens[f"{prec}_batched"] = p.cell_updates / (ms / 1000.0)
+        ens[f"{prec}_batched_shape"] = {k: tune[k] for k in ("variant", "rows_per_tile")}
+        b.close()
+        if prec == "fp64":  # the same members as plain FP64 runs, one after another
+            def solo():
+                u = 0
+                for dm, m in zip(doms, members):
+                    k, _ = dm.advance(args.ens_steps)
+                    u += k * m.interior_cells
+                return u
+            u, ms = _timed(stream, solo)
+            ens["fp64_sequential"] = u / (ms / 1000.0)
+        for dm in doms:
+            dm.close()
+    ens["fp32_batched_vs_fp64_batched"] = ens["fp32_batched"] / ens["fp64_batched"]
+    ens["fp32_batched_vs_fp64_sequential"] = ens["fp32_batched"] / ens["fp64_sequential"]
+    out["ensemble"] = ens
+    return out
+
+
+def serve_arm(args):
+    """Serving workload: Poisson arrivals of flood scenarios (side
+    log-uniform 512..4096, 0.5-6 h simulated, terrain/roughness/rain as the
+    ensemble workload, 20 % FP64 / 80 % FP32) admitted under a 150 GB HBM
+    budget.  Reports scenarios/hour, cell-updates/s and p50/p99 solve latency
+    (arrival to result) of the requests completed before the wall limit."""
+    import torch
+    from triton_b200.serving import Server, poisson_requests, summary
+    torch.cuda.set_device(0)
+    reqs = poisson_requests(rate=args.serve_rate, seconds=args.serve_seconds, seed=7)
+    limit = args.serve_max_wall or 2.0 * args.serve_seconds
+    srv = Server(hbm_budget=150e9, chunk_steps=32)
+    sampler = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+    sampler.start()
+    t0 = time.perf_counter()
+    srv.run(reqs, deadline=limit)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    s = summary(reqs, wall)
+    line = {"metric": "scenarios/hour", "value": s["scenarios_per_hour"], "unit": "scenarios/hour", "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "impl": "ours",
+            "config": {"workload": f"Poisson arrivals {args.serve_rate}/s for {args.serve_seconds:.0f} s, side "
+                                   "log-uniform 512..4096, 0.5-6 h simulated, 20% FP64 / 80% FP32, "
+                                   "150 GB HBM admission budget", "wall_limit_s": limit},
+            "serving": dict(s, peak_hbm_used_bytes=srv.peak_used, chunks=srv.chunks,
+                            unfinished=sum(r.finished is None for r in reqs),
+                            cell_updates_per_s_all_work=srv.cell_updates / wall),
+            "clocks": clocks}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,12 +297,23 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="", help="flux kernel launch shape 'variant:rows_per_tile' (skips autotune)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 and ensemble measurements")
+    ap.add_argument("--ens-members", type=int, default=64)
+    ap.add_argument("--ens-max-side", type=int, default=1024)
+    ap.add_argument("--ens-steps", type=int, default=100)
+    ap.add_argument("--serve-seconds", type=float, default=600.0, help="serve: arrival window (s)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="serve: Poisson arrival rate (1/s)")
+    ap.add_argument("--serve-max-wall", type=float, default=0.0, help="serve: stop after this many s (0: window x 2)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "serve":
+        if rank == 0:
+            serve_arm(args)
+        return
     sc, desc = workload(args.workload, args.n)
 
     if args.impl == "reference":
@@ -309,6 +421,10 @@ def main():
             cpu = {"value": r[0], "unit": "cell-updates/s", "cores": threads, "kind": "reference",
                    "sample": f"{r[1]} time steps of the same workload, reference OpenMP build ({r[2]:.2f} s compute)"}
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms and args.precision == "fp64":
+        forms = measure_forms(args, sc, stream, value)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -334,6 +450,8 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
         }
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line))
     d.close()
     if world > 1:

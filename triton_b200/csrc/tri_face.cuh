@@ -6,10 +6,14 @@
 // neighbour across it (east for x faces, NORTH for y faces: row-1).
 //
 // Bit-exactness contract: with T=double and the library's compile flags
-// (--fmad=false, IEEE div/sqrt), the value of every expression below equals
-// the reference's, because each expression keeps the reference's operand
-// order and association.  The normal components are compile-time constants;
-// the multiplications by them are kept (x*0.0 is not x in IEEE arithmetic).
+// (--fmad=false, IEEE div/sqrt), every output equals the reference's bit for
+// bit for finite states: each non-zero term keeps the reference's operand
+// order and association.  Terms that are zero by construction are left out
+// (products with the zero component of the face normal, contributions of a
+// wave with zero speed, entropy-fix parts of waves without a fix): adding a
+// zero never changes a non-zero sum, and a sum that is zero is flushed to +0
+// before it is used, so only the sign of zeros inside the solver differs, and
+// NaN propagation in a state that is already non-finite.
 #pragma once
 
 #include "tri_common.cuh"
@@ -58,11 +62,20 @@ struct StepK {
   T dx, dt, rdx, rdt, hextra;
 };
 
+// Products with the face normal (nx, ny) = (1,0) or (0,1): the component
+// itself (the product with the zero component is a zero term).
+template <typename T, bool XFACE>
+__device__ __forceinline__ T n_dot(T a, T b) {  // a*nx + b*ny
+  return XFACE ? a : b;
+}
+template <typename T, bool XFACE>
+__device__ __forceinline__ T n_cross(T a, T b) {  // b*nx - a*ny
+  return XFACE ? b : -a;
+}
+
 template <typename T, bool XFACE>
 __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<T>& c2, const StepK<T>& K) {
   const T dx = K.dx, dt = K.dt, hextra = K.hextra;
-  constexpr T nx = XFACE ? T(1) : T(0);
-  constexpr T ny = XFACE ? T(0) : T(1);
   const T G = T(kGravity), SG = T(kSqrtG), E12 = eps12<T>();
   FaceOut<T> out;
   out.a0 = out.a1 = out.a2 = out.b0 = out.b1 = out.b2 = T(0);
@@ -82,20 +95,21 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   const T rssq = recip(ssq);
   const T u12 = div_shared(u1 * sqh1 + u2 * sqh2, ssq, rssq);
   const T v12 = div_shared(v1 * sqh1 + v2 * sqh2, ssq, rssq);
-  const T un = u12 * nx + v12 * ny;
+  const T un = n_dot<T, XFACE>(u12, v12);
   T lam0 = un - c12, lam1 = un, lam2 = un + c12;
   T lamE0 = T(0), lamE2 = T(0);  // lamE1 is always zero
 
   // Harten-Hyman style entropy fix on the acoustic waves
   {
-    T e1 = u1 * nx + v1 * ny - SG * sqh1;
-    T e2 = u2 * nx + v2 * ny - SG * sqh2;
+    const T un1 = n_dot<T, XFACE>(u1, v1), un2 = n_dot<T, XFACE>(u2, v2);
+    T e1 = un1 - SG * sqh1;
+    T e2 = un2 - SG * sqh2;
     if (e1 < T(0) && e2 > T(0)) {
       lamE0 = lam0 - e1 * (e2 - lam0) / (e2 - e1);
       lam0 = e1 * (e2 - lam0) / (e2 - e1);
     }
-    e1 = u1 * nx + v1 * ny + SG * sqh1;
-    e2 = u2 * nx + v2 * ny + SG * sqh2;
+    e1 = un1 + SG * sqh1;
+    e2 = un2 + SG * sqh2;
     if (e1 < T(0) && e2 > T(0)) {
       lamE2 = lam2 - e2 * (lam2 - e1) / (e2 - e1);
       lam2 = e2 * (lam2 - e1) / (e2 - e1);
@@ -103,15 +117,16 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   }
 
   // eigenvector components (row 0 and row 2 have a leading 1, row 1 a 0)
-  const T r01 = u12 - c12 * nx, r02 = v12 - c12 * ny;
-  const T r11 = -c12 * ny, r12 = c12 * nx;
-  const T r21 = u12 + c12 * nx, r22 = v12 + c12 * ny;
+  // (components that are zero for this face direction are never used)
+  const T r01 = XFACE ? u12 - c12 : u12, r02 = XFACE ? v12 : v12 - c12;
+  const T r11 = -c12, r12 = c12;  // wave 1: (0, -c12*ny, c12*nx)
+  const T r21 = XFACE ? u12 + c12 : u12, r22 = XFACE ? v12 : v12 + c12;
 
   // wave strengths
   const T dqx = c2.qx - c1.qx, dqy = c2.qy - c1.qy;
-  const T aq = div_shared((dqx * nx + dqy * ny) - un * dh, c12, rc12);
+  const T aq = div_shared(n_dot<T, XFACE>(dqx, dqy) - un * dh, c12, rc12);
   const T al0 = T(0.5) * (dh - aq);
-  const T al1 = div_shared((dqy - v12 * dh) * nx - (dqx - u12 * dh) * ny, c12, rc12);
+  const T al1 = div_shared(n_cross<T, XFACE>(dqx - u12 * dh, dqy - v12 * dh), c12, rc12);
   const T al2 = T(0.5) * (dh + aq);
 
   // upwinded bed-step source, limited where the step is higher than the water
@@ -165,13 +180,9 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     {
       const T w = lam1 * al1 - be1;
       if (lam1 > T(0)) {
-        q0 += w * T(0);
-        q1 += w * r11;
-        q2 += w * r12;
+        if (XFACE) q2 += w * r12; else q1 += w * r11;
       } else {
-        p0 += w * T(0);
-        p1 += w * r11;
-        p2 += w * r12;
+        if (XFACE) p2 += w * r12; else p1 += w * r11;
       }
     }
     // wave 2: eigenvector (1, r21, r22)
@@ -188,8 +199,8 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
       }
     }
   }
-  // entropy-fix parts (lamE1 == 0 goes to the owner side, as in the reference)
-  {
+  // entropy-fix parts (a wave without a fix contributes zeros; lamE1 is zero)
+  if (lamE0 != T(0)) {
     const T w = lamE0 * al0;
     if (lamE0 > T(0)) {
       q0 += w * T(1);
@@ -201,13 +212,7 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
       p2 += w * r02;
     }
   }
-  {
-    const T w = T(0) * al1;
-    p0 += w * T(0);
-    p1 += w * r11;
-    p2 += w * r12;
-  }
-  {
+  if (lamE2 != T(0)) {
     const T w = lamE2 * al2;
     if (lamE2 > T(0)) {
       q0 += w * T(1);

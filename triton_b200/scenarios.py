@@ -274,7 +274,7 @@ def watershed(n=8192, dx=10.0, seed=1234, duration=6 * 3600.0, rain_mm_h=50.0, r
 
 
 def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0, 20.0), duration=3 * 3600.0,
-             rain_range=(10.0, 100.0), rain_hours=1.0, manning_spread=0.3, max_side=None):
+             rain_range=(10.0, 100.0), rain_hours=1.0, manning_spread=0.3, max_side=None, gpu_noise=False):
     """Ensemble of rain-on-grid watershed members of uneven sizes: per member
     a side drawn log-uniformly in [side_min, side_max] (capped at max_side),
     a cell size in dx_range, a rain intensity in rain_range (mm/h) for
@@ -290,7 +290,7 @@ def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0,
         rain = float(rng.uniform(*rain_range))
         mann = 0.035 * (1.0 + float(rng.uniform(-manning_spread, manning_spread)))
         sc = watershed(n=side, dx=dx, seed=int(rng.integers(1 << 31)), duration=duration, rain_mm_h=rain,
-                       rain_hours=rain_hours, manning_median=mann, nsrc=0)
+                       rain_hours=rain_hours, manning_median=mann, nsrc=0, gpu_noise=gpu_noise)
         sc.name = f"member{i:03d}"
         out.append(sc)
     return out

@@ -126,9 +126,11 @@ class Server:
             b.set_members(doms)
 
     # -- loop ------------------------------------------------------------------
-    def run(self, requests, clock=time.perf_counter, idle_sleep=0.002):
+    def run(self, requests, clock=time.perf_counter, idle_sleep=0.002, deadline=None):
         """Serves `requests` (arrival times relative to the start) until all
-        are done; returns them with admission/finish times filled in."""
+        are done, or until `deadline` seconds after the start (requests not
+        finished by then keep finished=None); returns them with admission and
+        finish times filled in."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
         t0 = clock()
@@ -137,6 +139,8 @@ class Server:
         try:
             while pending or waiting or any(self.live.values()):
                 t = now()
+                if deadline is not None and t > deadline:
+                    break
                 while pending and pending[0].arrival <= t:
                     waiting.append(pending.popleft())
                 running = [p for p in ("fp64", "fp32") if self.live[p]]
