@@ -166,7 +166,7 @@ int tri_domain_observe(tri_domain* d, double* h, double* qx, double* qy);
 /* Sum of h over interior cells times dx^2, accumulated in FP64. */
 int tri_domain_volume(tri_domain* d, double* volume);
 int tri_domain_synchronize(tri_domain* d);
-/* Volume accounts (FP32 form; zeros in the FP64 form), m^3: out[0] interior
+/* Volume accounts (both forms), m^3: out[0] interior
  * volume now (FP64 sum), then the cumulative Kahan-compensated FP64 totals of
  * inflow through boundary faces, point sources, runoff, external-boundary
  * depth resets and negative-depth clipping since the last H upload.  Volume

@@ -17,11 +17,16 @@ template <typename T>
 __host__ __device__ constexpr T eps12();
 template <>
 __host__ __device__ constexpr double eps12<double>() { return 1e-12; }
-// The FP32 form keeps the FP64 thresholds: the reference's single-precision
-// build flushes flux contributions below 1e-6, which deletes the mass of thin
-// sheet flow; 1e-12 is still a normal float.
+// The FP32 form keeps the FP64 absolute threshold (the reference's
+// single-precision build flushes flux contributions below 1e-6, which deletes
+// the mass of thin sheet flow) and adds a relative one, kNoise32, for
+// contributions that are rounding noise of larger terms.
 template <>
 __host__ __device__ constexpr float eps12<float>() { return 1e-12f; }
+
+// FP32 form: relative size below which a face contribution is rounding noise
+// of the terms that formed it (about 17 float ulps).
+constexpr double kNoise32 = 2e-6;
 
 __device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
 // FP32 form: the approximate hardware square root, one PTX instruction, so it
@@ -82,6 +87,28 @@ __device__ __forceinline__ double div_shared(double a, double b, double y) {
 }
 // FP32 form: one multiplication (within 1.5 ulp).
 __device__ __forceinline__ float div_shared(float a, float, float y) { return a * y; }
+
+// Integer mix of a cell index and a step number (deterministic, so a batch
+// member rounds exactly as its solo run).
+__device__ __forceinline__ uint32_t cell_hash(uint32_t id, uint32_t step) {
+  uint32_t x = id * 0x9E3779B1u ^ (step * 0x85EBCA77u + 0x27D4EB2Fu);
+  x ^= x >> 15;
+  x *= 0x2C1B3C6Du;
+  x ^= x >> 12;
+  x *= 0x297A2D39u;
+  x ^= x >> 15;
+  return x;
+}
+
+// s rounded to one of its two neighbouring floats with probability
+// proportional to closeness (unbiased: E[result] = s), r uniform in [0, 2^32).
+// s - a and b - a are exact in FP64.
+__device__ __forceinline__ float round_stochastic(double s, uint32_t r) {
+  const float a = __double2float_rd(s), b = __double2float_ru(s);
+  if (a == b) return a;
+  const double u = (double)r * 0x1p-32;
+  return (s - (double)a) > u * ((double)b - (double)a) ? b : a;
+}
 
 // Reciprocal of a divisor shared by several quotients.  FP64: RN(1/b), as
 // div_shared requires.  FP32 form: the hardware's approximate reciprocal

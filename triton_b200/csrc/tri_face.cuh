@@ -23,18 +23,22 @@ namespace tri {
 // Cell quantities every face of a cell uses, computed once per cell:
 // velocities are zero below hextra (kernels_flux.h:98-117) and sqrt(h) is the
 // reference's SQRTH array (kernels.h:178).
+// z is the bed level (FP64 form) or the cell's FP32 offset from zb, the FP64
+// base level of its 32x32 tile (FP32 form; zb is unused in FP64).
 template <typename T>
 struct CellQ {
   T h, qx, qy, z, sq, u, v;
+  double zb;
 };
 
 template <typename T>
-__device__ __forceinline__ CellQ<T> make_cell(T h, T qx, T qy, T z, T hextra) {
+__device__ __forceinline__ CellQ<T> make_cell(T h, T qx, T qy, T z, T hextra, double zb = 0.0) {
   CellQ<T> c;
   c.h = h;
   c.qx = qx;
   c.qy = qy;
   c.z = z;
+  c.zb = zb;
   c.sq = dev_fmax(dev_sqrt(h), T(0));
   if (h >= hextra) {
     const T rh = recip(h);
@@ -130,15 +134,28 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   const T al2 = T(0.5) * (dh + aq);
 
   // upwinded bed-step source, limited where the step is higher than the water
-  const T z1 = c1.z, z2 = c2.z;
-  const T dz = z2 - z1;
+  T dz;
+  bool above1, above2;  // z1 + h1 < z2, z2 + h2 < z1
+  if (sizeof(T) == 8) {
+    const T z1 = c1.z, z2 = c2.z;
+    dz = z2 - z1;
+    above1 = z1 + h1 < z2;
+    above2 = z2 + h2 < z1;
+  } else {
+    // FP32 form: the bed step from each cell's own (base, offset) pair, so
+    // every evaluation of a face gets the same value (a face on a tile edge
+    // is evaluated by both tiles, and mass is conserved only if both agree)
+    dz = c1.zb == c2.zb ? c2.z - c1.z : (T)((c2.zb - c1.zb) + ((double)c2.z - (double)c1.z));
+    above1 = h1 < dz;
+    above2 = h2 < -dz;
+  }
   T dzp = dz, hp;
   if (dz >= T(0)) {
     hp = h1;
-    if (z1 + h1 < z2) dzp = h1;
+    if (above1) dzp = h1;
   } else {
     hp = h2;
-    if (z2 + h2 < z1) dzp = -h2;
+    if (above2) dzp = -h2;
   }
   T be0 = div_shared(T(0.5) * G * (hp - T(0.5) * dev_fabs(dzp)) * dzp, c12, rc12);
 
@@ -225,12 +242,24 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     }
   }
   // flush tiny contributions, then scale to depth/discharge increments
-  if (dev_fabs(p0) < E12) p0 = T(0);
-  if (dev_fabs(q0) < E12) q0 = T(0);
-  if (dev_fabs(p1) < E12) p1 = T(0);
-  if (dev_fabs(q1) < E12) q1 = T(0);
-  if (dev_fabs(p2) < E12) p2 = T(0);
-  if (dev_fabs(q2) < E12) q2 = T(0);
+  T th0 = E12, th1 = E12;
+  if (sizeof(T) == 4) {
+    // FP32 form: a contribution within the rounding noise of the terms that
+    // formed it is zero.  1e-12 lies far above FP64 noise but far below FP32
+    // noise: at a shoreline the fluctuation into a dry cell cancels to FP32
+    // noise (~1e-9), which would leave 1e-11 m of water there, make the cell
+    // count as wet and let water climb the bank.
+    const T s0 = dev_fabs(lam0 * al0) + dev_fabs(be0) + dev_fabs(lam2 * al2) + dev_fabs(lamE0 * al0) +
+                 dev_fabs(lamE2 * al2);
+    th0 = dev_fmax(E12, T(kNoise32) * s0);
+    th1 = dev_fmax(E12, T(kNoise32) * (s0 * (dev_fabs(u12) + dev_fabs(v12) + c12) + dev_fabs(lam1 * al1) * c12));
+  }
+  if (dev_fabs(p0) < th0) p0 = T(0);
+  if (dev_fabs(q0) < th0) q0 = T(0);
+  if (dev_fabs(p1) < th1) p1 = T(0);
+  if (dev_fabs(q1) < th1) q1 = T(0);
+  if (dev_fabs(p2) < th1) p2 = T(0);
+  if (dev_fabs(q2) < th1) q2 = T(0);
   out.a0 = div_by_rcp(dt * p0, dx, K.rdx);
   out.a1 = div_by_rcp(dt * p1, dx, K.rdx);
   out.a2 = div_by_rcp(dt * p2, dx, K.rdx);

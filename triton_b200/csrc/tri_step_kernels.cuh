@@ -195,6 +195,8 @@ struct FluxCtx {
   const T* rates;
   int rows, cols, rb, nstrips;
   int nroff, roff_rows, roff_row;
+  uint32_t step;  // it_count of the running step (seeds the FP32 form's rounding of runoff)
+  double dtd;     // the step's dt in FP64
   StepK<T> K;
 };
 
@@ -222,6 +224,8 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   X.nroff = clk->nroff;
   X.roff_rows = clk->roff_rows;
   X.roff_row = clk->runoff_row;
+  X.step = (uint32_t)clk->it_count;
+  X.dtd = clk->global_dt;
   X.K.dx = dx;
   X.K.dt = T(clk->global_dt);
   X.K.rdx = rdx;
@@ -250,10 +254,8 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   const bool upd = mid && c >= 1 && c <= cols - 2;
   const bool gcol = incol && (c == 0 || c == cols - 1);  // ghost column owned by this lane
   const bool owner = incol && (mid || gcol);
-  constexpr bool kAcct = sizeof(T) == 4;  // FP32 form keeps the FP64 volume accounts
+  constexpr bool kAcct = true;  // FP64 volume accounts in both forms
   double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
-  // bed levels relative to the base of the tile's first cell
-  const double zref = X.bed.ref_of(r0, min(sx * kStripCols + 1, cols - 1));
 
   auto copy_ghost = [&](int r) {
     const size_t id = (size_t)r * cols + c;
@@ -264,17 +266,19 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
 
   // raw values of the next row are loaded one iteration ahead
   T lh = T(0), lqx = T(0), lqy = T(0), lz = T(0);
+  double lzb = 0.0;
   auto fetch = [&](int r) {
     if (incol) {
       const size_t id = (size_t)r * cols + c;
       lh = hi[id];
       lqx = qxi[id];
       lqy = qyi[id];
-      lz = X.bed.local(id, r, c, zref);
+      lz = X.bed.z[id];  // FP32 form: the offset from the base of the cell's tile
+      lzb = X.bed.base_at(r, c);
     }
   };
   fetch(r0 - 1);
-  CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra);
+  CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra, lzb);
   if (r0 - 1 == 0 && owner) copy_ghost(0);
   fetch(r0);
   RowParts<T> pp;
@@ -282,7 +286,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   T pn2 = T(0);  // Manning of the previous row's cell
 
   for (int r = r0; r <= r1 + 1; ++r) {
-    const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra);
+    const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra, lzb);
     T cn2 = T(0);
     if (r <= r1) {
       if (upd) cn2 = X.n2[(size_t)r * cols + c];
@@ -312,7 +316,15 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       if (X.nroff > 0) {  // update_runoff (kernels.h:128-149)
         const T h0 = hn;
         const T net = X.rates[(size_t)X.zone[id] * X.roff_rows + X.roff_row];
-        hn += net * dt;
+        if (sizeof(T) == 8) {
+          hn += net * dt;
+        } else if (net != T(0)) {
+          // FP32 form: uniform rain adds the same increment to every cell of
+          // a zone, so rounding h + r*dt to nearest would round the same way
+          // in every cell of a binade; the FP64 sum is rounded
+          // stochastically instead (unbiased), deterministic in (cell, step)
+          hn = (T)round_stochastic((double)hn + (double)net * X.dtd, cell_hash((uint32_t)id, X.step));
+        }
         if (hn < hextra) {
           if (hn < T(0)) hn = T(0);
           qn = T(0);
@@ -337,6 +349,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
     left.sq = shfl_up1(cur.sq);
     left.u = shfl_up1(cur.u);
     left.v = shfl_up1(cur.v);
+    left.zb = sizeof(T) == 4 ? __shfl_up_sync(0xffffffffu, cur.zb, 1) : 0.0;
     FaceOut<T> Xf;
     Xf.a0 = Xf.a1 = Xf.a2 = Xf.b0 = Xf.b1 = Xf.b2 = T(0);
     if (lane >= 1 && incol && c >= 1) Xf = face_flux<T, true>(left, cur, X.K);
@@ -415,7 +428,7 @@ __global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int
   const T hs = (flow * dt) / (dx * dx);
   hij += hs;
   h[sid] = hij;
-  if (sizeof(T) == 4) atomicAdd(&clk->acc_step[kAccSources], (double)hs);
+  atomicAdd(&clk->acc_step[kAccSources], (double)hs);
 }
 
 template <typename T>
@@ -554,8 +567,8 @@ __device__ __forceinline__ void extbc_apply(DevClock* __restrict__ clk, const St
       hij = dev_fmax(aux - (T)bed.absolute(ii, ix, iy), T(0));
     } else {  // FP32 form: level minus bed in FP64, then rounded
       hij = (T)fmax((double)aux - bed.absolute(ii, ix, iy), 0.0);
-      atomicAdd(&clk->acc_step[kAccExtbc], (double)hij - (double)h[ii]);
     }
+    atomicAdd(&clk->acc_step[kAccExtbc], (double)hij - (double)h[ii]);
   } else {
     const T aux = var1[s0];
     T vel = T(0);
@@ -888,7 +901,7 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
                                                         int cols, int band, double dx, double cn, T hextra,
                                                         float* __restrict__ arrival, float arrival_depth) {
   if (WETDRY && !clk->active) return;
-  if (sizeof(T) == 4 && WETDRY && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  if (WETDRY && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
   const unsigned long long key = wetdry_band<T, WETDRY>(clk, sb, bed, maxh, rows, cols, band, dx, cn, hextra,
                                                         arrival, arrival_depth, blockIdx.x, blockIdx.y);
   block_min_into(key, &clk->dt_key[WETDRY ? clk->wr : clk->rd]);
@@ -901,7 +914,7 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
                                                             float arrival_depth) {
   extern __shared__ __align__(128) unsigned char wet_smem[];
   if (!clk->active) return;
-  if (sizeof(T) == 4 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
   const unsigned long long key = wetdry_staged<T>(clk, sb, bed, maxh, rows, cols, hextra, arrival, arrival_depth,
                                                   blockIdx.x, blockIdx.y, reinterpret_cast<T*>(wet_smem));
   block_min_into(key, &clk->dt_key[clk->wr]);
@@ -947,7 +960,7 @@ __global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* _
   DevClock* clk = M.clk;
   if (!clk->active) return;
   const uint32_t local = blockIdx.x - M.wet_begin;
-  if (sizeof(T) == 4 && local == 0 && threadIdx.x == 0) fold_accounts(clk);
+  if (local == 0 && threadIdx.x == 0) fold_accounts(clk);
   const unsigned long long key =
       wetdry_staged<T>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, M.hextra, M.arrival, M.arrival_depth,
                        (int)(local % M.wet_nbx), (int)(local / M.wet_nbx), reinterpret_cast<T*>(wet_smem));
@@ -981,7 +994,7 @@ __global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2
   const T hs = (flow * dt) / (M.dx * M.dx);
   hij += hs;
   h[sid] = hij;
-  if (sizeof(T) == 4) atomicAdd(&clk->acc_step[kAccSources], (double)hs);
+  atomicAdd(&clk->acc_step[kAccSources], (double)hs);
 }
 
 template <typename T>

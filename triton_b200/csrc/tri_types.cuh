@@ -36,7 +36,7 @@ struct DevClock {
   unsigned long long dt_key[2];
   const double* roff_t;
   const double* hyg_t;
-  // FP32 form: FP64 volume accounting in depth units (multiply by dx^2).
+  // FP64 volume accounting in depth units (multiply by dx^2), both forms.
   // acc_step collects the running step (atomics), the wet-dry kernel folds it
   // into the Kahan-compensated totals acc_sum/acc_comp.
   double acc_step[kAccTerms];
@@ -71,6 +71,7 @@ struct BedMap<double> {
   __device__ __forceinline__ double ref_of(int, int) const { return 0.0; }
   __device__ __forceinline__ double local(size_t id, int, int, double) const { return z[id]; }
   __device__ __forceinline__ double local_v(double zv, int, int, double) const { return zv; }
+  __device__ __forceinline__ double base_at(int, int) const { return 0.0; }
   __device__ __forceinline__ double absolute(size_t id, int, int) const { return z[id]; }
 };
 template <>
@@ -83,6 +84,7 @@ struct BedMap<float> {
     const double b = base[(r >> 5) * ntc + (c >> 5)];
     return b == ref ? z[id] : z[id] + (float)(b - ref);
   }
+  __device__ __forceinline__ double base_at(int r, int c) const { return base[(r >> 5) * ntc + (c >> 5)]; }
   // the same for an offset already read (from shared memory)
   __device__ __forceinline__ float local_v(float zv, int r, int c, double ref) const {
     const double b = base[(r >> 5) * ntc + (c >> 5)];

@@ -56,8 +56,14 @@ def compare(sc, duration=None, arrival_depth=0.1, fixed_dt=None):
     both = (ta >= 0) & (tb >= 0)
     terr = np.abs(tb[both] - ta[both])
     bal = b["balance"]
-    accounts = sum(bal[k] for k in ("boundary", "sources", "runoff", "extbc", "clipping"))
+    terms = ("boundary", "sources", "runoff", "extbc", "clipping")
+    accounts = sum(bal[k] for k in terms)
     resid = (b["volume"] - b["v0"] - accounts) / max(abs(b["volume"]), 1e-300)
+    resid64 = (a["volume"] - a["v0"] - sum(a["balance"][k] for k in terms)) / max(abs(a["volume"]), 1e-300)
+    # where the volumes part: each account of the FP32 run minus the FP64 run's
+    # (forcing totals differ with the time levels: runoff and sources apply
+    # over whole steps, so the step that crosses a table time decides them)
+    dacc = {k: b["balance"][k] - a["balance"][k] for k in terms}
     return dict(
         steps_fp64=a["steps"], steps_fp32=b["steps"], simtime=a["simtime"],
         max_depth_error_m=float(err.max()), rms_depth_error_m=float(np.sqrt(np.mean(err ** 2))),
@@ -69,5 +75,7 @@ def compare(sc, duration=None, arrival_depth=0.1, fixed_dt=None):
         arrival_cells=int(both.sum()), arrival_mismatch_cells=int(((ta >= 0) != (tb >= 0)).sum()),
         volume_fp64=a["volume"], volume_fp32=b["volume"],
         volume_rel_error=abs(b["volume"] - a["volume"]) / max(abs(a["volume"]), 1e-300),
-        mass_balance_residual=float(resid), accounts_fp32=bal,
+        mass_balance_residual=float(resid), mass_balance_residual_fp64=float(resid64),
+        accounts_fp32=bal, accounts_fp64=a["balance"],
+        account_differences=dacc,
     )
