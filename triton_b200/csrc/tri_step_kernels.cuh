@@ -135,12 +135,35 @@ struct RowParts {  // rhs contributions collected for one cell
 
 template <typename T>
 __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>& p, T s0, T s1, T s2, T n2v, T dt,
-                                            T hextra, T& ho, T& qxo, T& qyo) {
+                                            T hextra, T& ho, T& qxo, T& qyo, double& clip, uint32_t rnd) {
   const T E12 = eps12<T>();
   const T G = T(kGravity);
   const T hn = c.h;
-  const T rh0 = p.e0 + p.n0, rh1 = p.w0 + s0;
-  T hij = hn - rh0 - rh1;
+  T hij;
+  if (sizeof(T) == 8) {
+    const T rh0 = p.e0 + p.n0, rh1 = p.w0 + s0;
+    hij = hn - rh0 - rh1;
+    clip = hij < T(0) ? -(double)hij : 0.0;
+  } else {
+    // FP32 form: the depth change is summed in FP64 and rounded
+    // stochastically (unbiased).  Rounded to nearest, a deep cell drops every
+    // inflow below half its ulp while the thin cell it came from loses it
+    // exactly, so runoff draining from films into channels would vanish
+    // (1.4e-5 of the volume over 2 h of rain on a 2048^2 watershed).  A
+    // result within the rounding noise of its terms is zero, as FP32
+    // arithmetic would give it: noise must not leave water on a cell that
+    // drained, or the cell counts as wet.
+    const double sd = (double)hn - (((double)p.e0 + (double)p.n0) + ((double)p.w0 + (double)s0));
+    const double noise = kNoise32 * ((double)hn + (double)dev_fabs(p.e0) + (double)dev_fabs(p.n0) +
+                                     (double)dev_fabs(p.w0) + (double)dev_fabs(s0));
+    if (sd <= noise) {
+      clip = -sd;  // depth removed (noise) or clipped back to zero, both accounted
+      hij = T(0);
+    } else {
+      clip = 0.0;
+      hij = (T)round_stochastic(sd, rnd);
+    }
+  }
   T qxij, qyij;
   if (hij < T(0)) hij = T(0);
   if (hij < hextra) {
@@ -298,7 +321,9 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
     if (r - 1 >= r0 && upd) {
       const size_t id = (size_t)(r - 1) * cols + c;
       T hn, qn, vn;
-      update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn);
+      double clip;
+      update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn, clip,
+                     cell_hash((uint32_t)id, 2u * X.step));
       if (kAcct) {
         // Inflow through faces shared with ghost cells, in depth units.  The
         // update is in fluctuation form, so the mass flux through a face of
@@ -310,8 +335,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
         if (c == cols - 2) acc_b -= (double)pp.e0 + sxq * (double)prev.qx;
         if (r - 1 == 1) acc_b -= (double)pp.n0 + sxq * (double)prev.qy;
         if (r - 1 == rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
-        const T raw = prev.h - (pp.e0 + pp.n0) - (pp.w0 + Y.b0);
-        if (raw < T(0)) acc_c -= (double)raw;
+        acc_c += clip;
       }
       if (X.nroff > 0) {  // update_runoff (kernels.h:128-149)
         const T h0 = hn;
@@ -323,7 +347,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
           // a zone, so rounding h + r*dt to nearest would round the same way
           // in every cell of a binade; the FP64 sum is rounded
           // stochastically instead (unbiased), deterministic in (cell, step)
-          hn = (T)round_stochastic((double)hn + (double)net * X.dtd, cell_hash((uint32_t)id, X.step));
+          hn = (T)round_stochastic((double)hn + (double)net * X.dtd, cell_hash((uint32_t)id, 2u * X.step + 1u));
         }
         if (hn < hextra) {
           if (hn < T(0)) hn = T(0);

@@ -21,6 +21,7 @@ result is bit-for-bit the one the scenario gets alone.
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import time
 from dataclasses import dataclass, field
 from typing import Callable
@@ -59,7 +60,14 @@ class Request:
 
 
 class Server:
-    def __init__(self, hbm_budget=150e9, chunk_steps=32, max_members=512, shapes=None):
+    """`prefetch` requests at the head of the waiting queue have their inputs
+    built on host threads while the GPU steps (a request carries a builder,
+    not arrays; building is the client's work and runs off the loop)."""
+
+    def __init__(self, hbm_budget=150e9, chunk_steps=32, max_members=512, shapes=None, prefetch=6,
+                 build_threads=4):
+        self.prefetch = int(prefetch)
+        self.build_threads = int(build_threads)
         self.budget = float(hbm_budget)
         self.chunk = int(chunk_steps)
         self.max_members = int(max_members)
@@ -72,20 +80,28 @@ class Server:
         self.cell_updates = 0
 
     # -- admission ---------------------------------------------------------------
+    @staticmethod
+    def _ready(r):
+        fut = getattr(r, "_future", None)
+        return fut is None or fut.done()
+
     def _fits(self, r):
         if not r.footprint:
             if not r.rows:
-                sc = r.build()
+                fut = getattr(r, "_future", None)
+                sc = fut.result() if fut is not None else r.build()
                 r.rows, r.cols = sc.rows, sc.cols
-                r._sc = sc
+                r._sc, r._future = sc, None
             r.footprint = Domain.footprint(r.rows, r.cols, r.precision)
         if r.footprint > self.budget:
             raise ValueError(f"request {r.rid}: footprint {r.footprint} B exceeds the budget {self.budget:.0f} B")
         return self.used + r.footprint <= self.budget and len(self.live[r.precision]) < self.max_members
 
     def _admit(self, r, now):
-        sc = getattr(r, "_sc", None) or r.build()
+        fut = getattr(r, "_future", None)
+        sc = getattr(r, "_sc", None) or (fut.result() if fut is not None else r.build())
         r._sc = None
+        r._future = None
         d = sc.to_domain(r.precision)
         # no intermediate outputs: the request wants its final state
         d.set_clock(print_interval=sc.sim_duration, print_observation=sc.sim_duration, time_series=0,
@@ -133,6 +149,7 @@ class Server:
         finish times filled in."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
+        pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.build_threads) if self.prefetch > 0 else None
         t0 = clock()
         now = lambda: clock() - t0  # noqa: E731
         dirty = set()
@@ -146,8 +163,14 @@ class Server:
                 running = [p for p in ("fp64", "fp32") if self.live[p]]
                 for p in running:
                     self.batches[p].launch(self.chunk)
-                # admit while the GPU steps (arrival order, head of line first)
-                while waiting and self._fits(waiting[0]):
+                # inputs of the next waiting requests are built on host threads
+                if pool is not None:
+                    for r in list(waiting)[:self.prefetch]:
+                        if getattr(r, "_future", None) is None and getattr(r, "_sc", None) is None:
+                            r._future = pool.submit(r.build)
+                # admit while the GPU steps (arrival order, head of line first;
+                # a head whose inputs are still being built waits for them)
+                while waiting and self._ready(waiting[0]) and self._fits(waiting[0]):
                     r = waiting.popleft()
                     self._admit(r, now())
                     dirty.add(r.precision)
@@ -164,7 +187,11 @@ class Server:
                 dirty.clear()
                 if not running and not waiting and pending:
                     time.sleep(min(idle_sleep, max(pending[0].arrival - now(), 0.0)))
+                elif not running and waiting:  # inputs still being built
+                    time.sleep(idle_sleep)
         finally:
+            if pool is not None:
+                pool.shutdown(wait=True, cancel_futures=True)
             for p, b in self.batches.items():
                 b.close()
             self.batches.clear()
