@@ -254,8 +254,21 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     th0 = dev_fmax(E12, T(kNoise32) * s0);
     th1 = dev_fmax(E12, T(kNoise32) * (s0 * (dev_fabs(u12) + dev_fabs(v12) + c12) + dev_fabs(lam1 * al1) * c12));
   }
-  if (dev_fabs(p0) < th0) p0 = T(0);
-  if (dev_fabs(q0) < th0) q0 = T(0);
+  if (sizeof(T) == 4 && th0 > E12) {
+    // FP32 form: a mass contribution that is noise moves to the other side
+    // instead of vanishing, so the face still conserves mass; the dry side of
+    // a shoreline face gets exactly nothing
+    const bool np = dev_fabs(p0) < th0, nq = dev_fabs(q0) < th0;
+    if (nq && (!np || h1 >= h2)) {  // both noise: to the side with more water
+      p0 += q0;
+      q0 = T(0);
+    } else if (np) {
+      q0 += p0;
+      p0 = T(0);
+    }
+  }
+  if (dev_fabs(p0) < E12) p0 = T(0);
+  if (dev_fabs(q0) < E12) q0 = T(0);
   if (dev_fabs(p1) < th1) p1 = T(0);
   if (dev_fabs(q1) < th1) q1 = T(0);
   if (dev_fabs(p2) < th1) p2 = T(0);
