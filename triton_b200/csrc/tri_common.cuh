@@ -100,14 +100,20 @@ __device__ __forceinline__ uint32_t cell_hash(uint32_t id, uint32_t step) {
   return x;
 }
 
-// s rounded to one of its two neighbouring floats with probability
-// proportional to closeness (unbiased: E[result] = s), r uniform in [0, 2^32).
-// s - a and b - a are exact in FP64.
-__device__ __forceinline__ float round_stochastic(double s, uint32_t r) {
-  const float a = __double2float_rd(s), b = __double2float_ru(s);
-  if (a == b) return a;
-  const double u = (double)r * 0x1p-32;
-  return (s - (double)a) > u * ((double)b - (double)a) ? b : a;
+// a + b rounded stochastically between its two neighbouring floats
+// (unbiased), computed in FP32: the rounding error of a + b is exact by
+// Knuth's TwoSum, and the sum moves to the neighbour on the error's side with
+// probability |error| / gap.  r uniform in [0, 2^32).  *exact_lo receives the
+// error, so (double)RN(a + b) + error is the exact sum.
+__device__ __forceinline__ float sr_add(float a, float b, uint32_t r, float* exact_lo) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  const float err = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  *exact_lo = err;
+  if (err == 0.0f) return s;
+  const float t = nextafterf(s, err > 0.0f ? INFINITY : -INFINITY);
+  const float u = (float)(r >> 8) * 0x1p-24f;
+  return u * fabsf(t - s) < fabsf(err) ? t : s;
 }
 
 // Reciprocal of a divisor shared by several quotients.  FP64: RN(1/b), as

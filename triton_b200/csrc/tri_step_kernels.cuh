@@ -153,15 +153,16 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     // result within the rounding noise of its terms is zero, as FP32
     // arithmetic would give it: noise must not leave water on a cell that
     // drained, or the cell counts as wet.
-    const double sd = (double)hn - (((double)p.e0 + (double)p.n0) + ((double)p.w0 + (double)s0));
-    const double noise = kNoise32 * ((double)hn + (double)dev_fabs(p.e0) + (double)dev_fabs(p.n0) +
-                                     (double)dev_fabs(p.w0) + (double)dev_fabs(s0));
-    if (sd <= noise) {
-      clip = -sd;  // depth removed (noise) or clipped back to zero, both accounted
+    const float parts = (p.e0 + p.n0) + (p.w0 + s0);
+    float lo;
+    const float hs = sr_add(hn, -parts, rnd, &lo);
+    const float noise = float(kNoise32) * (hn + dev_fabs(p.e0) + dev_fabs(p.n0) + dev_fabs(p.w0) + dev_fabs(s0));
+    if (__fadd_rn(hn, -parts) <= noise) {
+      clip = -((double)__fadd_rn(hn, -parts) + (double)lo);  // removed (noise) or clipped to zero: accounted
       hij = T(0);
     } else {
       clip = 0.0;
-      hij = (T)round_stochastic(sd, rnd);
+      hij = hs;
     }
   }
   T qxij, qyij;
@@ -219,7 +220,6 @@ struct FluxCtx {
   int rows, cols, rb, nstrips;
   int nroff, roff_rows, roff_row;
   uint32_t step;  // it_count of the running step (seeds the FP32 form's rounding of runoff)
-  double dtd;     // the step's dt in FP64
   StepK<T> K;
 };
 
@@ -248,7 +248,6 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   X.roff_rows = clk->roff_rows;
   X.roff_row = clk->runoff_row;
   X.step = (uint32_t)clk->it_count;
-  X.dtd = clk->global_dt;
   X.K.dx = dx;
   X.K.dt = T(clk->global_dt);
   X.K.rdx = rdx;
@@ -347,7 +346,8 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
           // a zone, so rounding h + r*dt to nearest would round the same way
           // in every cell of a binade; the FP64 sum is rounded
           // stochastically instead (unbiased), deterministic in (cell, step)
-          hn = (T)round_stochastic((double)hn + (double)net * X.dtd, cell_hash((uint32_t)id, 2u * X.step + 1u));
+          float lo;
+          hn = sr_add(hn, net * dt, cell_hash((uint32_t)id, 2u * X.step + 1u), &lo);
         }
         if (hn < hextra) {
           if (hn < T(0)) hn = T(0);
