@@ -748,15 +748,19 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
 
 // ---------------------------------------------------------------------------
 // Staged wet-dry/dt: one block per band of WetStage<T>::kBand rows x
-// kWetCols columns.  The block first stages, in shared memory, its rows of h
-// and the bed with a halo row above and below, and its rows of qx, qy and the
+// kWetCols columns.  The block stages, in shared memory, its rows of h and
+// the bed with a halo row above and below, and its rows of qx, qy and the
 // maximum depth, each row from column c0-1 to c0+kWetCols (clipped to the
 // grid) with one bulk asynchronous copy (cp.async.bulk: rounded out to
-// 16-byte boundaries, which every field's kFieldPad allows at its end), all
-// completing on one mbarrier, so a block has its whole tile in flight at
-// once.  The FP32 form then turns the staged bed offsets into levels relative
-// to one reference in place (one conversion per staged cell).  Then each
-// thread walks one column down the band from shared memory.
+// 16-byte boundaries, which every field's kFieldPad allows at its end).  All
+// copies are issued at once, in groups of two output rows, each group
+// completing on its own mbarrier: a thread walking its column down the band
+// starts on the first two rows while the later rows are still in flight, so
+// a block's loads overlap its own arithmetic even when every block of a wave
+// starts at the same moment.  The FP32 form turns a staged bed offset into a
+// level relative to the block's reference as it reads it (its tile's delta,
+// added in registers), so no pass over shared memory and no block barrier
+// sits between the copies and the arithmetic.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct WetStage {
@@ -766,8 +770,32 @@ struct WetStage {
   static constexpr int kHRows = kBand + 2;                           // h and bed rows (with halos)
   static constexpr int kRows = 2 * kHRows + 3 * kBand;               // + qx, qy, max depth rows
   static constexpr size_t kData = (size_t)kRows * kCap * sizeof(T);
-  static constexpr size_t kBytes = kData + 16 + 4 * kHRows;          // + mbarrier + row offsets
+  // copy groups: group 0 = h and bed staged rows 0-3 and band rows 0-1 of
+  // qx, qy, max depth (14 rows); group g > 0 = h and bed staged rows 2g+2,
+  // 2g+3 and band rows 2g, 2g+1 (10 rows)
+  static constexpr int kGroups = kBand / 2;
+  static constexpr int kFirst = 14, kNext = 10;
+  static constexpr size_t kBarBytes = (8 * kGroups + 15) / 16 * 16;
+  // FP32 form: the staged rows span at most 2 x 6 bed tiles of 32 x 32
+  // (kBand + 2 <= 32 rows, kWetCols + 2 <= 5 * 32 + 2 columns)
+  static constexpr int kTileCols = 6, kTileSlots = 2 * kTileCols;
+  static constexpr size_t kBytes = kData + kBarBytes + 4 * kHRows + 4 * kTileSlots;  // + row offsets, tiles
 };
+static_assert(kStageBand<double> % 2 == 0 && kStageBand<float> % 2 == 0, "bands are whole copy groups");
+static_assert(WetStage<double>::kFirst + (WetStage<double>::kGroups - 1) * WetStage<double>::kNext ==
+                  WetStage<double>::kRows, "copy groups cover the staged rows");
+static_assert(WetStage<float>::kFirst + (WetStage<float>::kGroups - 1) * WetStage<float>::kNext ==
+                  WetStage<float>::kRows, "copy groups cover the staged rows");
+static_assert(WetStage<float>::kBand + 2 <= 32, "staged rows span at most two bed tile rows");
+
+// Gives up on a block whose copies did not land: reports it, waits (bounded)
+// once more on every group from 'from' on so no copy still writes this
+// block's shared memory when it exits.
+template <int kGroups>
+__device__ __forceinline__ void stage_abandon(DevClock* clk, uint64_t* bar, int from) {
+  atomicExch(&clk->status, kStatusStageTimeout);
+  for (int g = from; g < kGroups; ++g) mbar_wait(&bar[g], 0);
+}
 
 template <typename T>
 __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict__ clk, const StateBufs<T>& sb,
@@ -775,6 +803,7 @@ __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict
                                                             int cols, T hextra, float* __restrict__ arrival,
                                                             float arrival_depth, int bx, int by, T* stage) {
   using S = WetStage<T>;
+  constexpr bool kF32 = sizeof(T) == 4;
   const int buf = clk->dst;
   T* __restrict__ qx = sb.QX(buf);
   T* __restrict__ qy = sb.QY(buf);
@@ -784,120 +813,174 @@ __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict
   const int ra = by * S::kBand;
   const int rz = min(ra + S::kBand - 1, rows - 1);
   const int cl = max(c0 - 1, 0), ce = min(c0 + kWetCols + 1, cols);  // staged columns [cl, ce)
-  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(stage) + S::kData);
+  unsigned char* tail = reinterpret_cast<unsigned char*>(stage) + S::kData;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tail);
   // offs[j]: column c of staged row ra-1+j sits at buffer index c + offs[j]
-  int* offs = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(stage) + S::kData + 16);
-  if (tid == 0) mbar_init(bar, 1);
+  int* offs = reinterpret_cast<int*>(tail + S::kBarBytes);
+  // FP32 form: per bed tile the staged rows touch, its base minus the
+  // block's reference level
+  float* tdel = reinterpret_cast<float*>(offs + S::kHRows);
+  const int rlo = max(ra - 1, 0), rhi = min(rz + 1, rows - 1);
+  const int tr0 = rlo >> 5, tc0 = cl >> 5;
+  if (tid < S::kGroups) mbar_init(&bar[tid], 1);
   if (tid < S::kHRows) {
     const int64_t r = (int64_t)(ra - 1 + tid);
     offs[tid] = (int)(r * cols - ((r * cols + cl) & ~(int64_t)(S::kVec - 1)));
   }
+  if (kF32 && tid >= 32 && tid < 32 + S::kTileSlots) {
+    const int s = tid - 32, tr = tr0 + s / S::kTileCols, tc = tc0 + s % S::kTileCols;
+    if (tr <= (rhi >> 5) && tc <= ((ce - 1) >> 5))
+      tdel[s] = (float)(bed.base_at(tr << 5, tc << 5) - bed.ref_of(ra, min(c0, cols - 1)));
+  }
   __syncthreads();
   if (tid < 32) {
-    for (int k = lane; k < S::kRows; k += 32) {
-      const T* src;
-      int r;
-      if (k < 2 * S::kHRows) {
-        r = ra - 1 + (k < S::kHRows ? k : k - S::kHRows);
-        src = k < S::kHRows ? (const T*)sb.H(buf) : (const T*)bed.z;
-        if (r < 0 || r > rows - 1) continue;
+    for (int i = lane; i < S::kRows; i += 32) {
+      // copy i -> group g, field f (0 h, 1 bed, 2 qx, 3 qy, 4 max depth) and
+      // q: staged row (h, bed; global row ra-1+q) or band row (global ra+q)
+      int g, f, q;
+      if (i < S::kFirst) {
+        g = 0;
+        if (i < 8) {
+          f = i >> 2;
+          q = i & 3;
+        } else {
+          f = 2 + ((i - 8) >> 1);
+          q = (i - 8) & 1;
+        }
       } else {
-        const int q = k - 2 * S::kHRows, f = q / S::kBand;
-        r = ra + (q - f * S::kBand);
-        src = f == 0 ? (const T*)qx : (f == 1 ? (const T*)qy : (const T*)maxh);
+        const int t = (i - S::kFirst) % S::kNext;
+        g = 1 + (i - S::kFirst) / S::kNext;
+        if (t < 4) {
+          f = t >> 1;
+          q = 2 * g + 2 + (t & 1);
+        } else {
+          f = 2 + ((t - 4) >> 1);
+          q = 2 * g + (t & 1);
+        }
+      }
+      int r, slot;
+      const T* src;
+      if (f < 2) {
+        r = ra - 1 + q;
+        if (r < 0 || r > rows - 1) continue;
+        slot = f * S::kHRows + q;
+        src = f == 0 ? (const T*)sb.H(buf) : (const T*)bed.z;
+      } else {
+        r = ra + q;
         if (r > rz) continue;
+        slot = 2 * S::kHRows + (f - 2) * S::kBand + q;
+        src = f == 2 ? (const T*)qx : (f == 3 ? (const T*)qy : (const T*)maxh);
       }
       const int64_t e0 = ((int64_t)r * cols + cl) & ~(int64_t)(S::kVec - 1);
       const int64_t e1 = ((int64_t)r * cols + ce + S::kVec - 1) & ~(int64_t)(S::kVec - 1);
       const uint32_t bytes = (uint32_t)((e1 - e0) * (int64_t)sizeof(T));
-      mbar_expect_tx(bar, bytes);
-      bulk_g2s(stage + (size_t)k * S::kCap, src + e0, bytes, bar);
+      mbar_expect_tx(&bar[g], bytes);
+      bulk_g2s(stage + (size_t)slot * S::kCap, src + e0, bytes, &bar[g]);
     }
     __syncwarp();
-    if (lane == 0) mbar_arrive(bar);
+    if (lane == 0)
+      for (int g = 0; g < S::kGroups; ++g) mbar_arrive(&bar[g]);
   }
-  if (!mbar_wait(bar, 0)) {
-    // a copy never completed: report it, wait (bounded) once more so no copy
-    // still writes this block's shared memory when it exits, contribute nothing
-    atomicExch(&clk->status, kStatusStageTimeout);
-    mbar_wait(bar, 0);
-    return kDtKeyInf;
-  }
-  T* sh = stage;
-  T* sz = stage + (size_t)S::kHRows * S::kCap;
+  const T* sh = stage;
+  const T* sz = stage + (size_t)S::kHRows * S::kCap;
   const T* sqx = stage + (size_t)2 * S::kHRows * S::kCap;
   const T* sqy = sqx + (size_t)S::kBand * S::kCap;
   const T* smh = sqy + (size_t)S::kBand * S::kCap;
-  const double zref = bed.ref_of(ra, min(c0, cols - 1));
-  if (sizeof(T) == 4) {  // bed offsets -> levels relative to zref, in place
-    const int w = ce - cl;
-    for (int e = tid; e < S::kHRows * w; e += kWetCols) {
-      const int j = e / w, c = cl + (e - j * w), r = ra - 1 + j;
-      if (r < 0 || r > rows - 1) continue;
-      T& zv = sz[(size_t)j * S::kCap + c + offs[j]];
-      zv = (T)bed.local_v(zv, r, c, zref);
-    }
-    __syncthreads();
-  }
   const int c = c0 + tid;
   const bool incol = c < cols;
   const bool intcol = c >= 1 && c <= cols - 2;
+  // FP32 form: tile deltas of columns c-1, c, c+1 in tile rows 0 and 1
+  // (BedMap::local_v; where a delta is zero the level is the offset itself,
+  // up to the sign of a zero, which no comparison below sees)
+  T dw0 = T(0), dw1 = T(0), dc0 = T(0), dc1 = T(0), de0 = T(0), de1 = T(0);
+  if (kF32 && intcol) {
+    const int tw = ((c - 1) >> 5) - tc0, tc = (c >> 5) - tc0, te = ((c + 1) >> 5) - tc0;
+    dw0 = (T)tdel[tw];
+    dc0 = (T)tdel[tc];
+    de0 = (T)tdel[te];
+    if ((rhi >> 5) > tr0) {
+      dw1 = (T)tdel[S::kTileCols + tw];
+      dc1 = (T)tdel[S::kTileCols + tc];
+      de1 = (T)tdel[S::kTileCols + te];
+    }
+  }
   const float simtime_now = (float)clk->simtime;
-  unsigned long long key = kDtKeyInf;
+  // largest wave speed of the thread's cells (NaN speeds left out, as
+  // speed_key does); one key at the end equals the minimum of per-cell keys
+  T dmax = T(-1);
   if (incol) {
+    // bed level of the thread's column at staged row j (buffer offset oj)
+    auto zlev = [&](int j, int oj) -> T {
+      T v = sz[j * S::kCap + c + oj];
+      if (kF32) v += (((ra - 1 + j) >> 5) > tr0) ? dc1 : dc0;
+      return v;
+    };
     int om = offs[0], o = offs[1];
+    T zm = T(0), z0 = T(0);
 #pragma unroll
     for (int jq = 0; jq < S::kBand; ++jq) {
       const int r = ra + jq;
       if (r > rz) break;
+      if ((jq & 1) == 0 && !mbar_wait(&bar[jq >> 1], 0)) {
+        stage_abandon<S::kGroups>(clk, bar, jq >> 1);
+        return kDtKeyInf;
+      }
       const int j = jq + 1;
       const int op = offs[j + 1];
+      if (jq == 0) {
+        zm = zlev(0, om);
+        z0 = zlev(1, o);
+      }
+      const T zp = zlev(j + 1, op);
       const size_t id = (size_t)r * cols + c;
-      const T* hrow = sh + (size_t)j * S::kCap + o;
+      const T* hrow = sh + j * S::kCap + o;
       const T hij = hrow[c];
-      T qxv = sqx[(size_t)jq * S::kCap + c + o], qyv = sqy[(size_t)jq * S::kCap + c + o];
+      T qxv = sqx[jq * S::kCap + c + o], qyv = sqy[jq * S::kCap + c + o];
       if (intcol && r >= 1 && r <= rows - 2) {
-        const T* zrow = sz + (size_t)j * S::kCap + o;
-        const T zij = zrow[c];
         if (hij > hextra) {
           const T he = hrow[c + 1], hw = hrow[c - 1];
-          const T hm = sh[(size_t)(j - 1) * S::kCap + c + om];
-          const T hp = sh[(size_t)(j + 1) * S::kCap + c + op];
-          const T ze = zrow[c + 1], zw = zrow[c - 1];
-          const T zm = sz[(size_t)(j - 1) * S::kCap + c + om];
-          const T zp = sz[(size_t)(j + 1) * S::kCap + c + op];
-          if ((hij + zij < ze && he < E12) || (hij + zij < zw && hw < E12)) {
+          const T hm = sh[(j - 1) * S::kCap + c + om];
+          const T hp = sh[(j + 1) * S::kCap + c + op];
+          const T* zrow = sz + j * S::kCap + o;
+          T ze = zrow[c + 1], zw = zrow[c - 1];
+          if (kF32) {
+            const bool t1 = (r >> 5) > tr0;
+            ze += t1 ? de1 : de0;
+            zw += t1 ? dw1 : dw0;
+          }
+          if ((hij + z0 < ze && he < E12) || (hij + z0 < zw && hw < E12)) {
             qxv = T(0);
             qx[id] = T(0);
           }
-          if ((hij + zij < zm && hm < E12) || (hij + zij < zp && hp < E12)) {
+          if ((hij + z0 < zm && hm < E12) || (hij + z0 < zp && hp < E12)) {
             qyv = T(0);
             qy[id] = T(0);
           }
         }
-        if (hij > smh[(size_t)jq * S::kCap + c + o]) maxh[id] = hij;
+        if (hij > smh[jq * S::kCap + c + o]) maxh[id] = hij;
         if (arrival != nullptr && hij > arrival_depth && !(arrival[id] < 3.0e38f)) arrival[id] = simtime_now;
       }
       if (hij > hextra) {  // wave speed of the CFL dt (reduced as its maximum)
-        double d;
+        T d;
         if (sizeof(T) == 8) {  // FP64: the reference's denominator, bit for bit
           const double hd = (double)hij;
           const double sq = fmax(sqrt(hd), 0.0);
           const double maxu = fmax(fabs((double)qxv), fabs((double)qyv)) / hd;
-          d = maxu + kSqrtG * sq;
+          d = (T)(maxu + kSqrtG * sq);
         } else {  // FP32 form: speed in FP32, maximum and dt in FP64
           const T sq = dev_fmax(dev_sqrt(hij), T(0));
           const T maxu = fdiv(dev_fmax(dev_fabs(qxv), dev_fabs(qyv)), hij);
-          d = (double)(maxu + T(kSqrtG) * sq);
+          d = maxu + T(kSqrtG) * sq;
         }
-        const unsigned long long k = speed_key(d);
-        key = k < key ? k : key;
+        dmax = dev_fmax(dmax, d);
       }
+      zm = z0;
+      z0 = zp;
       om = o;
       o = op;
     }
   }
-  return key;
+  return dmax >= T(0) ? speed_key((double)dmax) : kDtKeyInf;
 }
 
 // Block minimum of the threads' keys, folded into *slot with one atomic.
