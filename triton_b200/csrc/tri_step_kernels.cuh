@@ -753,8 +753,8 @@ __device__ __forceinline__ unsigned long long wetdry_band(const DevClock* __rest
 // maximum depth, each row from column c0-1 to c0+kWetCols (clipped to the
 // grid) with one bulk asynchronous copy (cp.async.bulk: rounded out to
 // 16-byte boundaries, which every field's kFieldPad allows at its end).  All
-// copies are issued at once, in groups of two output rows, each group
-// completing on its own mbarrier: a thread walking its column down the band
+// copies are issued at once, in groups of kStageGroupRows output rows, each
+// group completing on its own mbarrier: a thread walking its column down the band
 // starts on the first two rows while the later rows are still in flight, so
 // a block's loads overlap its own arithmetic even when every block of a wave
 // starts at the same moment.  The FP32 form turns a staged bed offset into a
@@ -770,18 +770,20 @@ struct WetStage {
   static constexpr int kHRows = kBand + 2;                           // h and bed rows (with halos)
   static constexpr int kRows = 2 * kHRows + 3 * kBand;               // + qx, qy, max depth rows
   static constexpr size_t kData = (size_t)kRows * kCap * sizeof(T);
-  // copy groups: group 0 = h and bed staged rows 0-3 and band rows 0-1 of
-  // qx, qy, max depth (14 rows); group g > 0 = h and bed staged rows 2g+2,
-  // 2g+3 and band rows 2g, 2g+1 (10 rows)
-  static constexpr int kGroups = kBand / 2;
-  static constexpr int kFirst = 14, kNext = 10;
+  // copy groups of kGR output rows: group 0 = h and bed staged rows
+  // 0..kGR+1 and band rows 0..kGR-1 of qx, qy, max depth; group g > 0 = h and
+  // bed staged rows g*kGR+2..g*kGR+kGR+1 and band rows g*kGR..g*kGR+kGR-1
+  static constexpr int kGR = kStageGroupRows<T>;
+  static constexpr int kGroups = kBand / kGR;
+  static constexpr int kFirst = 2 * (kGR + 2) + 3 * kGR, kNext = 5 * kGR;
   static constexpr size_t kBarBytes = (8 * kGroups + 15) / 16 * 16;
   // FP32 form: the staged rows span at most 2 x 6 bed tiles of 32 x 32
   // (kBand + 2 <= 32 rows, kWetCols + 2 <= 5 * 32 + 2 columns)
   static constexpr int kTileCols = 6, kTileSlots = 2 * kTileCols;
   static constexpr size_t kBytes = kData + kBarBytes + 4 * kHRows + 4 * kTileSlots;  // + row offsets, tiles
 };
-static_assert(kStageBand<double> % 2 == 0 && kStageBand<float> % 2 == 0, "bands are whole copy groups");
+static_assert(kStageBand<double> % kStageGroupRows<double> == 0 && kStageBand<float> % kStageGroupRows<float> == 0,
+              "bands are whole copy groups");
 static_assert(WetStage<double>::kFirst + (WetStage<double>::kGroups - 1) * WetStage<double>::kNext ==
                   WetStage<double>::kRows, "copy groups cover the staged rows");
 static_assert(WetStage<float>::kFirst + (WetStage<float>::kGroups - 1) * WetStage<float>::kNext ==
@@ -840,22 +842,22 @@ __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict
       int g, f, q;
       if (i < S::kFirst) {
         g = 0;
-        if (i < 8) {
-          f = i >> 2;
-          q = i & 3;
+        if (i < 2 * (S::kGR + 2)) {
+          f = i / (S::kGR + 2);
+          q = i % (S::kGR + 2);
         } else {
-          f = 2 + ((i - 8) >> 1);
-          q = (i - 8) & 1;
+          f = 2 + (i - 2 * (S::kGR + 2)) / S::kGR;
+          q = (i - 2 * (S::kGR + 2)) % S::kGR;
         }
       } else {
         const int t = (i - S::kFirst) % S::kNext;
         g = 1 + (i - S::kFirst) / S::kNext;
-        if (t < 4) {
-          f = t >> 1;
-          q = 2 * g + 2 + (t & 1);
+        if (t < 2 * S::kGR) {
+          f = t / S::kGR;
+          q = g * S::kGR + 2 + t % S::kGR;
         } else {
-          f = 2 + ((t - 4) >> 1);
-          q = 2 * g + (t & 1);
+          f = 2 + (t - 2 * S::kGR) / S::kGR;
+          q = g * S::kGR + (t - 2 * S::kGR) % S::kGR;
         }
       }
       int r, slot;
@@ -921,8 +923,8 @@ __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict
     for (int jq = 0; jq < S::kBand; ++jq) {
       const int r = ra + jq;
       if (r > rz) break;
-      if ((jq & 1) == 0 && !mbar_wait(&bar[jq >> 1], 0)) {
-        stage_abandon<S::kGroups>(clk, bar, jq >> 1);
+      if (jq % S::kGR == 0 && !mbar_wait(&bar[jq / S::kGR], 0)) {
+        stage_abandon<S::kGroups>(clk, bar, jq / S::kGR);
         return kDtKeyInf;
       }
       const int j = jq + 1;

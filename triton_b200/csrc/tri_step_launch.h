@@ -29,9 +29,12 @@ template <>
 struct FluxBudget<float> {
   static constexpr int v0 = 5, v1 = 6, v2 = 8;
 };
-// rows per block of the staged wet-dry/dt kernel (its shared-memory tile)
+// rows per block of the staged wet-dry/dt kernel (its shared-memory tile),
+// and output rows per group of its copies (each group on its own mbarrier)
 template <typename T>
 constexpr int kStageBand = sizeof(T) == 8 ? 4 : 8;
+template <typename T>
+constexpr int kStageGroupRows = 2;
 
 struct StepArgs {
   DevClock* clk;
