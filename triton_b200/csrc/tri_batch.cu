@@ -235,6 +235,7 @@ int prepare_members(tri_batch* b, int* runnable) {
   *runnable = 0;
   for (tri_domain* d : b->members) {
     DevClock* m = d->mirror;
+    d->tz_dirty = true;  // batched steps keep no dry-tile flags
     const bool live = m->simtime < m->sim_duration;
     m->halt = live ? 0 : 1;
     m->events = 0;

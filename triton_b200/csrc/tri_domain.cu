@@ -208,7 +208,62 @@ StepArgs step_args(tri_domain* d) {
   a.n_bc_waves = d->bc_waves.empty() ? 0 : (int)d->bc_waves.size() - 1;
   a.arrival = d->arrival;
   a.arrival_depth = d->arrival_depth;
+  a.tzero = d->tz_on ? d->tzero : nullptr;
+  a.tzero_wet = (d->maxh_nonneg && (d->arrival == nullptr || d->arrival_depth >= 0.0f)) ? a.tzero : nullptr;
   return a;
+}
+
+// Resets the dry-tile flags of the flux kernel for the current tile shape
+// (nothing is known to be zero, so the next two steps compute every tile)
+// and marks the tiles that must never be skipped: those holding a source or
+// an external boundary cell, and the edge tiles when the open boundaries
+// rewrite the ghost ring.  Runoff reaches every cell, so a domain with runoff
+// computes every tile.  Called outside graph capture, before steps.
+int reset_tiles(tri_domain* d) {
+  const int rows = d->desc.rows, cols = d->desc.cols;
+  const int64_t ns = (cols - 2 + kStripCols - 1) / kStripCols, nty = (rows - 2 + d->rb - 1) / d->rb;
+  const int64_t nt = ns * nty;
+  d->tz_dirty = false;
+  d->tz_on = d->nroff == 0;
+  if (!d->tz_on) return TRI_OK;
+  if (nt > d->tz_cap) {
+    drop_graph(d);  // the graphs hold the old flag pointer
+    free_devp(d->tzero);
+    d->tz_cap = 0;
+    if (cudaMalloc((void**)&d->tzero, 3 * (size_t)nt) != cudaSuccess) {
+      d->tz_on = false;
+      return set_error(TRI_E_NOMEM, "cudaMalloc of %lld tile flags failed", (long long)(3 * nt));
+    }
+    d->tz_cap = nt;
+  }
+  if (nt != d->tz_tiles) drop_graph(d);  // the pinned table moved
+  d->tz_tiles = nt;
+  std::vector<uint8_t>& pin = d->tz_pin_host;
+  pin.assign((size_t)nt, 0);
+  auto pin_cell = [&](int64_t id) {
+    const int r = (int)(id / cols), c = (int)(id % cols);
+    const int64_t ry = std::min<int64_t>(std::max(r - 1, 0) / d->rb, nty - 1);
+    const int64_t sx = std::min<int64_t>(std::max(c - 1, 0) / kStripCols, ns - 1);
+    pin[(size_t)(ry * ns + sx)] = 1;
+  };
+  if (d->nsrc > 0) {
+    std::vector<int32_t> cells(d->nsrc);
+    TRI_CUDA_TRY(cudaMemcpy(cells.data(), d->src_cells, d->nsrc * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int32_t id : cells) pin_cell(id);
+  }
+  if (d->nbc > 0) {
+    std::vector<int32_t> cells(d->nbc);
+    TRI_CUDA_TRY(cudaMemcpy(cells.data(), d->bc_cells, d->nbc * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int32_t id : cells) pin_cell(id);
+  }
+  if (d->desc.open_boundaries)
+    for (int64_t ry = 0; ry < nty; ry++)
+      for (int64_t sx = 0; sx < ns; sx++)
+        if (ry == 0 || ry == nty - 1 || sx == 0 || sx == ns - 1) pin[(size_t)(ry * ns + sx)] = 1;
+  TRI_CUDA_TRY(cudaMemsetAsync(d->tzero, 0, 2 * (size_t)nt, d->stream));
+  TRI_CUDA_TRY(cudaMemcpyAsync(d->tzero + 2 * nt, pin.data(), (size_t)nt, cudaMemcpyHostToDevice, d->stream));
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));  // 'pin' may be reassigned before the copy ran
+  return TRI_OK;
 }
 
 // Grid of the flux kernel for the domain's variant and tile height: one
@@ -433,6 +488,7 @@ int tri_domain_destroy(tri_domain* d) {
   if (!d) return TRI_OK;
   if (d->stream) cudaStreamSynchronize(d->stream);
   drop_graph(d);
+  free_devp(d->tzero);
   for (int i = 0; i < 2; i++) {
     free_dev(d->h[i]);
     free_dev(d->qx[i]);
@@ -480,6 +536,12 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   void* p = nullptr;
   int rc = field_ptr(d, field, &p);
   if (rc != TRI_OK) return rc;
+  if (field == TRI_FIELD_MAXH) {  // dry bands skip the wet-dry kernel only while no max depth is negative
+    bool nonneg = true;
+    for (int64_t i = 0; i < n && nonneg; i++) nonneg = host[i] >= 0.0;
+    if (nonneg != d->maxh_nonneg) drop_graph(d);
+    d->maxh_nonneg = nonneg;
+  }
   if (d->prec == TRI_FP64) {
     TRI_CUDA_TRY(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, d->stream));
   } else if (field == TRI_FIELD_DEM) {
@@ -506,6 +568,7 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   }
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
   if (field != TRI_FIELD_MAXH && field != TRI_FIELD_NMAN2) d->dt_valid = false;
+  d->tz_dirty = true;
   if (field == TRI_FIELD_H) {  // a new state restarts the volume accounts
     memset(d->mirror->acc_step, 0, sizeof(d->mirror->acc_step));
     memset(d->mirror->acc_sum, 0, sizeof(d->mirror->acc_sum));
@@ -542,6 +605,7 @@ int tri_domain_set_runoff(tri_domain* d, int32_t nzones, int32_t nrows, const do
                           const int32_t* zone_of_cell, int64_t ncells) {
   TRI_CHECK_ARG(d, "null domain");
   drop_graph(d);
+  d->tz_dirty = true;
   if (nzones <= 0) {
     d->nroff = 0;
     d->mirror->nroff = 0;
@@ -575,6 +639,7 @@ int tri_domain_set_sources(tri_domain* d, int32_t nsrc, const int32_t* cells, in
                            const double* flows) {
   TRI_CHECK_ARG(d, "null domain");
   drop_graph(d);
+  d->tz_dirty = true;
   if (nsrc <= 0) {
     d->nsrc = 0;
     d->mirror->nsrc = 0;
@@ -614,6 +679,7 @@ int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, co
                          const double* var2) {
   TRI_CHECK_ARG(d, "null domain");
   drop_graph(d);
+  d->tz_dirty = true;
   if (ncells <= 0) {
     d->nbc = 0;
     return TRI_OK;
@@ -744,6 +810,10 @@ int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* p) {
     if (rc != TRI_OK) return rc;
   }
   d->dt_valid = true;
+  if (d->tz_dirty) {
+    rc = reset_tiles(d);
+    if (rc != TRI_OK) return rc;
+  }
   // Chunks of steps, two in flight: after launching chunk k the host waits
   // for chunk k-1 and stops launching once a step has raised an event.
   const int chunk = 8;
@@ -862,6 +932,7 @@ int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out) {
       size_flux_grid(d);
       drop_graph(d);
       rc = save_restore(false);
+      if (rc == TRI_OK) rc = reset_tiles(d);  // the other buffer holds the last trial's state
       if (rc != TRI_OK) break;
       *m = saved;
       m->sim_duration = m->print_interval = m->print_observation = 1e300;
@@ -896,6 +967,7 @@ int tri_domain_autotune(tri_domain* d, int32_t trial_steps, tri_tuning* out) {
   int rc2 = save_restore(false);
   *m = saved;
   d->dt_valid = saved_valid;
+  d->tz_dirty = true;
   if (rc2 == TRI_OK) rc2 = push_clock(d);
   cudaStreamSynchronize(d->stream);
   cudaFree(bak);
@@ -924,6 +996,7 @@ int tri_domain_set_tuning(tri_domain* d, int32_t variant, int32_t rows_per_tile)
   d->rb = rows_per_tile;
   size_flux_grid(d);
   drop_graph(d);
+  d->tz_dirty = true;
   return TRI_OK;
 }
 

@@ -64,6 +64,15 @@ struct tri_domain {
   int vol_blocks = 0;
   // launch shape of the flux kernel (tile height, register variant, grid)
   int rb = 16, flux_blocks = 1, flux_variant = 0;
+  // dry-tile flags of the flux kernel for the current tile shape: [2][tiles]
+  // (tile holds only +0 in buffer 0 / 1) then [tiles] pinned.  Any change of
+  // state, forcing or shape outside the step kernels marks them dirty; they
+  // are reset (nothing known zero) before the next steps.
+  uint8_t* tzero = nullptr;
+  int64_t tz_cap = 0, tz_tiles = 0;
+  bool tz_on = false, tz_dirty = true;
+  bool maxh_nonneg = true;  // every max depth uploaded is >= 0
+  std::vector<uint8_t> tz_pin_host;
   double tuned_ms = 0;
   // graphs of 'graph_steps' steps
   cudaGraphExec_t graph = nullptr;

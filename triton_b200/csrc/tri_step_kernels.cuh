@@ -221,6 +221,13 @@ struct FluxCtx {
   int nroff, roff_rows, roff_row;
   uint32_t step;  // it_count of the running step (seeds the FP32 form's rounding of runoff)
   StepK<T> K;
+  // Dry-tile skipping (null: every tile is computed).  tz_src[t] / tz_dst[t]:
+  // tile t of the source / destination buffer holds only zero bits in h, qx
+  // and qy; tpin[t]: tile t is never skipped (a later kernel of the step
+  // writes into it: sources, external boundary cells, open boundaries).
+  const uint8_t* tz_src;
+  uint8_t* tz_dst;
+  const uint8_t* tpin;
 };
 
 template <typename T>
@@ -253,7 +260,33 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   X.K.rdx = rdx;
   X.K.rdt = T(clk->rdt);
   X.K.hextra = hextra;
+  X.tz_src = nullptr;
+  X.tz_dst = nullptr;
+  X.tpin = nullptr;
   return X;
+}
+
+// Zero bits (+0): a tile is skipped only where every value it would write
+// is +0 already, so skipping is exact.
+__device__ __forceinline__ bool nonzero_bits(double v) { return __double_as_longlong(v) != 0; }
+__device__ __forceinline__ bool nonzero_bits(float v) { return __float_as_uint(v) != 0u; }
+
+// A tile whose cells and whose four neighbour tiles' cells hold only +0 in
+// the source buffer computes exactly +0 everywhere (every face is dry-dry and
+// contributes nothing; no runoff on such a domain), and if its cells in the
+// destination buffer hold +0 already (it was all-zero two steps ago), it has
+// nothing to write.  Only lane 0's answer counts.
+template <typename T>
+__device__ __forceinline__ bool tile_skippable(const FluxCtx<T>& X, unsigned tile) {
+  if (X.tz_src == nullptr) return false;
+  const int ns = X.nstrips, nty = (X.rows - 2 + X.rb - 1) / X.rb;
+  const int sx = (int)(tile % ns), ry = (int)(tile / ns);
+  if (!(X.tz_src[tile] & X.tz_dst[tile]) || X.tpin[tile]) return false;
+  if (sx > 0 && !X.tz_src[tile - 1]) return false;
+  if (sx < ns - 1 && !X.tz_src[tile + 1]) return false;
+  if (ry > 0 && !X.tz_src[tile - ns]) return false;
+  if (ry < nty - 1 && !X.tz_src[tile + ns]) return false;
+  return true;
 }
 
 // One warp tile: strip sx (30 interior columns), rows r0..r1.
@@ -278,12 +311,16 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   const bool owner = incol && (mid || gcol);
   constexpr bool kAcct = true;  // FP64 volume accounts in both forms
   double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
+  const double sxq = (double)dt / (double)X.K.dx;  // dt/dx of the boundary discharges
 
+  bool wrote_nonzero = false;  // any value this lane writes is not +0
   auto copy_ghost = [&](int r) {
     const size_t id = (size_t)r * cols + c;
-    ho[id] = hi[id];
-    qxo[id] = qxi[id];
-    qyo[id] = qyi[id];
+    const T gh = hi[id], gqx = qxi[id], gqy = qyi[id];
+    ho[id] = gh;
+    qxo[id] = gqx;
+    qyo[id] = gqy;
+    wrote_nonzero |= nonzero_bits(gh) | nonzero_bits(gqx) | nonzero_bits(gqy);
   };
 
   // raw values of the next row are loaded one iteration ahead
@@ -329,7 +366,6 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
         // boundary cell i is F(Q_i).n plus the fluctuation it receives there:
         // west / south faces dt/dx*q - b, east / north faces -(a + dt/dx*q).
         // Also the depth the update clipped back to zero.
-        const double sxq = (double)dt / (double)X.K.dx;
         if (c == 1) acc_b += sxq * (double)prev.qx - (double)pp.w0;
         if (c == cols - 2) acc_b -= (double)pp.e0 + sxq * (double)prev.qx;
         if (r - 1 == 1) acc_b -= (double)pp.n0 + sxq * (double)prev.qy;
@@ -359,6 +395,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       ho[id] = hn;
       qxo[id] = qn;
       qyo[id] = vn;
+      wrote_nonzero |= nonzero_bits(hn) | nonzero_bits(qn) | nonzero_bits(vn);
     }
     if (r > r1) {
       if (r == rows - 1 && owner) copy_ghost(r);
@@ -400,22 +437,37 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       if (acc_c != 0.0) atomicAdd(&X.clk->acc_step[kAccClip], acc_c);
     }
   }
+  if (X.tz_dst != nullptr) {
+    const bool nz = __any_sync(0xffffffffu, wrote_nonzero);
+    if (lane == 0) X.tz_dst[tile] = (!nz && !X.tpin[tile]) ? 1 : 0;
+  }
 }
 
 template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                      const BedMap<T> bed, const T* __restrict__ n2,
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
-                                                     int rows, int cols, int rb, T dx, T rdx, T hextra) {
+                                                     int rows, int cols, int rb, T dx, T rdx, T hextra,
+                                                     uint8_t* __restrict__ tzero) {
   if (!clk->active) return;
-  const FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
+  FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
   const int lane = threadIdx.x & 31;
   const unsigned ntiles = (unsigned)X.nstrips * (unsigned)((rows - 2 + rb - 1) / rb);
+  if (tzero != nullptr) {  // [2][ntiles] zero flags by buffer, then [ntiles] pinned
+    X.tz_src = tzero + (size_t)clk->src * ntiles;
+    X.tz_dst = tzero + (size_t)clk->dst * ntiles;
+    X.tpin = tzero + 2 * (size_t)ntiles;
+  }
   while (true) {
     unsigned tile = 0;
-    if (lane == 0) tile = atomicAdd(&clk->tile_next, 1u);
+    int skip = 0;
+    if (lane == 0) {
+      tile = atomicAdd(&clk->tile_next, 1u);
+      skip = tile < ntiles && tile_skippable<T>(X, tile);
+    }
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
+    if (__shfl_sync(0xffffffffu, skip, 0)) continue;
     flux_tile<T>(X, tile, lane);
   }
 }
@@ -1016,14 +1068,39 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
   block_min_into(key, &clk->dt_key[WETDRY ? clk->wr : clk->rd]);
 }
 
+// True when every flux tile covering this block's band holds only +0 in the
+// step's destination buffer (tzero: the flux kernel's [2][tiles] flags).  A
+// band without a wet cell has nothing to mask, no wave speed, and (with max
+// depths and the arrival depth non-negative, which the host ensures before
+// it passes the flags) no max depth or arrival to record.  Cell (r, c)
+// belongs to tile row max(r-1,0)/rb and strip max(c-1,0)/kStripCols, clamped:
+// ghost rows and columns belong to the edge tiles that copy them.  Uniform
+// over the block.
+template <typename T>
+__device__ __forceinline__ bool band_all_zero(const DevClock* clk, const uint8_t* __restrict__ tzero, int rows,
+                                              int cols, int rb, int bx, int by) {
+  const int ns = (cols - 2 + kStripCols - 1) / kStripCols, nty = (rows - 2 + rb - 1) / rb;
+  const uint8_t* tz = tzero + (size_t)clk->dst * ((size_t)ns * nty);
+  const int ra = by * WetStage<T>::kBand, rz = min(ra + WetStage<T>::kBand - 1, rows - 1);
+  const int c0 = bx * kWetCols, c1 = min(c0 + kWetCols - 1, cols - 1);
+  const int t0 = min(max(ra - 1, 0) / rb, nty - 1), t1 = min(max(rz - 1, 0) / rb, nty - 1);
+  const int s0 = min(max(c0 - 1, 0) / kStripCols, ns - 1), s1 = min(max(c1 - 1, 0) / kStripCols, ns - 1);
+  const int nsx = s1 - s0 + 1, count = (t1 - t0 + 1) * nsx;
+  int nz = 0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) nz |= !tz[(size_t)(t0 + i / nsx) * ns + s0 + i % nsx];
+  return !__syncthreads_or(nz);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                             const BedMap<T> bed, T* __restrict__ maxh, int rows,
                                                             int cols, T hextra, float* __restrict__ arrival,
-                                                            float arrival_depth) {
+                                                            float arrival_depth, const uint8_t* __restrict__ tzero,
+                                                            int rb) {
   extern __shared__ __align__(128) unsigned char wet_smem[];
   if (!clk->active) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  if (tzero != nullptr && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) return;
   const unsigned long long key = wetdry_staged<T>(clk, sb, bed, maxh, rows, cols, hextra, arrival, arrival_depth,
                                                   blockIdx.x, blockIdx.y, reinterpret_cast<T*>(wet_smem));
   block_min_into(key, &clk->dt_key[clk->wr]);

@@ -47,7 +47,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   const BedMap<T> bed = bed_of<T>(a);
   k_clock<<<1, 32, 0, s>>>(a.clk);
   if (ev) cudaEventRecord(ev[0], s);
-#define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx
+#define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero
   switch (a.flux_variant) {
     case 0: k_flux_update<T, FluxBudget<T>::v0><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
     case 1: k_flux_update<T, FluxBudget<T>::v1><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
@@ -73,7 +73,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + WetStage<T>::kBand - 1) / WetStage<T>::kBand);
   if (ev) cudaEventRecord(ev[2], s);
   k_wetdry_staged<T><<<g2, kWetCols, WetStage<T>::kBytes, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, hx,
-                                                                 a.arrival, a.arrival_depth);
+                                                                 a.arrival, a.arrival_depth, a.tzero_wet, a.rb);
   if (ev) cudaEventRecord(ev[3], s);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;

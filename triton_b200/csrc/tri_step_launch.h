@@ -66,6 +66,11 @@ struct StepArgs {
   int n_bc_waves;
   float* arrival;
   float arrival_depth;
+  // dry-tile flags of the flux kernel ([2][tiles] by buffer + [tiles]
+  // pinned), or null to compute every tile; the same for the wet-dry kernel
+  // (null also while a max depth or the arrival depth is negative)
+  uint8_t* tzero;
+  const uint8_t* tzero_wet;
 };
 
 // One time step (clock, flux/update, sources, open ghosts, boundary cells,
