@@ -371,6 +371,7 @@ def main():
     clocks = sampler.stop()
     assert n_r == args.steps, (n_r, ev)
     flux_ms, flux_n, wet_ms, wet_n = d.get_timing()
+    flux_cells, wet_cells = d.get_work()  # interior cells the launches computed (dry tiles skipped)
     d.set_timing(False)
     t = torch.tensor([ms], device="cuda", dtype=torch.float64)
     if world > 1:
@@ -417,7 +418,11 @@ def main():
 
     peak, peak_kind = _peaks()
     flux_avg_s = (flux_ms / max(flux_n, 1)) / 1000.0
-    achieved = ALG_BYTES_FLUX[args.precision] * cells / flux_avg_s / 1e9
+    # algorithmic bytes of the cells one launch computed (a skipped dry tile
+    # moves nothing), and the same over every interior cell for comparison
+    flux_cells_launch = flux_cells / max(flux_n, 1)
+    achieved = ALG_BYTES_FLUX[args.precision] * flux_cells_launch / flux_avg_s / 1e9
+    achieved_all = ALG_BYTES_FLUX[args.precision] * cells / flux_avg_s / 1e9
     tpc = _traffic_per_cell("flux_update", args.precision)
     step_gbs = ALG_BYTES_STEP[args.precision] * cells * args.steps / (ms / 1000.0) / 1e9
 
@@ -447,7 +452,10 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_flux_update", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": (tpc * cells) if tpc is not None else None,
-                         "algorithmic_bytes_per_launch": ALG_BYTES_FLUX[args.precision] * cells,
+                         "algorithmic_bytes_per_launch": ALG_BYTES_FLUX[args.precision] * flux_cells_launch,
+                         "computed_cell_frac": flux_cells_launch / cells,
+                         "achieved_all_cells": achieved_all,
+                         "wetdry_computed_cell_frac": wet_cells / max(wet_n, 1) / cells,
                          "avg_launch_ms": flux_avg_s * 1000.0, "peak_source": f"MEASURED_PEAKS.json hbm_gbs "
                                                                                f"({peak_kind})",
                          "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,

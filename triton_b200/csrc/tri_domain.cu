@@ -1046,6 +1046,15 @@ int tri_domain_set_timing(tri_domain* d, int32_t enabled) {
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
   d->timing = enabled != 0;
   d->tev_used = 0;
+  d->mirror->work_flux = d->mirror->work_wet = 0;  // sent with the clock at the next advance
+  return TRI_OK;
+}
+
+int tri_domain_get_work(tri_domain* d, int64_t* flux_cells, int64_t* wetdry_cells) {
+  TRI_CHECK_ARG(d, "null domain");
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (flux_cells) *flux_cells = (int64_t)d->mirror->work_flux;
+  if (wetdry_cells) *wetdry_cells = (int64_t)d->mirror->work_wet;
   return TRI_OK;
 }
 

@@ -458,18 +458,24 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
     X.tz_dst = tzero + (size_t)clk->dst * ntiles;
     X.tpin = tzero + 2 * (size_t)ntiles;
   }
+  unsigned long long work = 0;  // interior cells of the tiles this warp computed (lane 0)
   while (true) {
     unsigned tile = 0;
     int skip = 0;
     if (lane == 0) {
       tile = atomicAdd(&clk->tile_next, 1u);
       skip = tile < ntiles && tile_skippable<T>(X, tile);
+      if (tile < ntiles && !skip) {
+        const int sx = (int)(tile % X.nstrips), r0 = 1 + (int)(tile / X.nstrips) * rb;
+        work += (unsigned long long)(min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols);
+      }
     }
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
     if (__shfl_sync(0xffffffffu, skip, 0)) continue;
     flux_tile<T>(X, tile, lane);
   }
+  if (lane == 0 && work) atomicAdd(&clk->work_flux, work);
 }
 
 // ---------------------------------------------------------------------------
@@ -1101,6 +1107,12 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
   if (!clk->active) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
   if (tzero != nullptr && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) return;
+  if (threadIdx.x == 0) {  // interior cells of this band
+    const int ra = max((int)blockIdx.y * WetStage<T>::kBand, 1);
+    const int rz = min((int)blockIdx.y * WetStage<T>::kBand + WetStage<T>::kBand - 1, rows - 2);
+    const int ca = max((int)blockIdx.x * kWetCols, 1), cz = min((int)blockIdx.x * kWetCols + kWetCols - 1, cols - 2);
+    if (rz >= ra && cz >= ca) atomicAdd(&clk->work_wet, (unsigned long long)(rz - ra + 1) * (cz - ca + 1));
+  }
   const unsigned long long key = wetdry_staged<T>(clk, sb, bed, maxh, rows, cols, hextra, arrival, arrival_depth,
                                                   blockIdx.x, blockIdx.y, reinterpret_cast<T*>(wet_smem));
   block_min_into(key, &clk->dt_key[clk->wr]);

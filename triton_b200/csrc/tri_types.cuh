@@ -42,6 +42,9 @@ struct DevClock {
   double acc_step[kAccTerms];
   double acc_sum[kAccTerms];
   double acc_comp[kAccTerms];
+  // interior cells of the flux tiles and wet-dry bands single-domain steps
+  // computed (dry tiles they skipped are not counted)
+  unsigned long long work_flux, work_wet;
 };
 
 template <typename T>

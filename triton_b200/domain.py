@@ -175,6 +175,13 @@ class Domain:
         check(lib().tri_domain_get_timing(self._h, C.byref(a), C.byref(na), C.byref(b), C.byref(nb)))
         return a.value, na.value, b.value, nb.value
 
+    def get_work(self):
+        """(flux cells, wet-dry cells) computed since set_timing: interior
+        cells of the tiles that were not skipped as dry."""
+        a, b = C.c_int64(), C.c_int64()
+        check(lib().tri_domain_get_work(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def autotune(self, trial_steps=10):
         """Times every flux-kernel launch shape on this domain's own state and
         keeps the fastest; the state and clock are restored afterwards."""
