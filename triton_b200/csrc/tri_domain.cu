@@ -113,6 +113,27 @@ __global__ void k_to_f64(const T* __restrict__ src, double* __restrict__ dst, in
 }
 
 // FP32 form: offsets of the bed from each 32x32 tile's FP64 base level.
+// Base level of each 32x32 tile (one block of 256 threads per tile): the
+// lowest interior cell of the tile (ghost cells hold walls or copies and must
+// not pull the base away from the terrain), 0 for a tile without interior
+// cells; NaN levels are passed over; a zero base is +0.
+__global__ void k_tile_base(const double* __restrict__ z, double* __restrict__ base, int rows, int cols, int ntc) {
+  const int tr = blockIdx.y, tc = blockIdx.x;
+  double m = 1e300;
+  for (int k = threadIdx.x; k < 32 * 32; k += blockDim.x) {
+    const int r = tr * 32 + (k >> 5), c = tc * 32 + (k & 31);
+    if (r >= 1 && r <= rows - 2 && c >= 1 && c <= cols - 2) m = fmin(m, z[(size_t)r * cols + c]);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmin(m, wm[w]);
+    base[(size_t)tr * ntc + tc] = (m == 1e300 || m == 0.0) ? 0.0 : m;
+  }
+}
+
 __global__ void k_bed_offsets(const double* __restrict__ z, const double* __restrict__ base, float* __restrict__ off,
                               int rows, int cols, int ntc) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,6 +186,14 @@ __global__ void k_volume_sum(const double* __restrict__ part, int n, double scal
   *out = acc * scale;
 }
 
+// *flag = 1 if any of the n values is negative or NaN (a zero of either sign is not).
+template <typename T>
+__global__ void k_flag_negative(const T* __restrict__ v, int64_t n, int32_t* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool neg = i < n && !(v[i] >= T(0));
+  if (__syncthreads_or(neg) && threadIdx.x == 0) atomicExch(flag, 1);
+}
+
 StepArgs step_args(tri_domain* d) {
   StepArgs a{};
   a.clk = d->clk;
@@ -209,7 +238,8 @@ StepArgs step_args(tri_domain* d) {
   a.arrival = d->arrival;
   a.arrival_depth = d->arrival_depth;
   a.tzero = d->tz_on ? d->tzero : nullptr;
-  a.tzero_wet = (d->maxh_nonneg && (d->arrival == nullptr || d->arrival_depth >= 0.0f)) ? a.tzero : nullptr;
+  a.tzero_wet = (d->arrival == nullptr || d->arrival_depth >= 0.0f) ? a.tzero : nullptr;
+  a.maxh_neg = d->maxh_neg;
   return a;
 }
 
@@ -468,6 +498,9 @@ int tri_domain_create(const tri_grid_desc* desc, void* stream, tri_domain** out)
   d->mirror->print_interval = 1e300;
   d->mirror->print_observation = 1e300;
   d->mirror->init_dt = 0.01;
+  if (cudaMalloc((void**)&d->maxh_neg, sizeof(int32_t)) != cudaSuccess)
+    return fail(set_error(TRI_E_CUDA, "flag allocation failed"));
+  cudaMemsetAsync(d->maxh_neg, 0, sizeof(int32_t), d->stream);
   d->vol_blocks = 296;
   if (cudaMalloc((void**)&d->vol_part, d->vol_blocks * sizeof(double)) != cudaSuccess ||
       cudaMalloc((void**)&d->vol_out, sizeof(double)) != cudaSuccess)
@@ -489,6 +522,7 @@ int tri_domain_destroy(tri_domain* d) {
   if (d->stream) cudaStreamSynchronize(d->stream);
   drop_graph(d);
   free_devp(d->tzero);
+  free_devp(d->maxh_neg);
   for (int i = 0; i < 2; i++) {
     free_dev(d->h[i]);
     free_dev(d->qx[i]);
@@ -536,34 +570,26 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
   void* p = nullptr;
   int rc = field_ptr(d, field, &p);
   if (rc != TRI_OK) return rc;
-  if (field == TRI_FIELD_MAXH) {  // dry bands skip the wet-dry kernel only while no max depth is negative
-    bool nonneg = true;
-    for (int64_t i = 0; i < n && nonneg; i++) nonneg = host[i] >= 0.0;
-    if (nonneg != d->maxh_nonneg) drop_graph(d);
-    d->maxh_nonneg = nonneg;
-  }
   if (d->prec == TRI_FP64) {
     TRI_CUDA_TRY(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, d->stream));
   } else if (field == TRI_FIELD_DEM) {
-    // base level of each 32x32 tile = its lowest interior cell (ghost cells
-    // hold walls or copies and must not pull the base away from the terrain)
+    // base level of each 32x32 tile = its lowest interior cell
     const int R = d->desc.rows, Cc = d->desc.cols;
-    std::vector<double> base((size_t)d->ntr * d->ntc, 1e300);
-    for (int r = 1; r < R - 1; r++)
-      for (int c = 1; c < Cc - 1; c++) {
-        double& b = base[(size_t)(r >> 5) * d->ntc + (c >> 5)];
-        b = std::min(b, host[(size_t)r * Cc + c]);
-      }
-    for (double& b : base)
-      if (b == 1e300) b = 0.0;
-    TRI_CUDA_TRY(cudaMemcpyAsync(d->zbase, base.data(), base.size() * 8, cudaMemcpyHostToDevice, d->stream));
     TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
+    k_tile_base<<<dim3((unsigned)d->ntc, (unsigned)d->ntr), 256, 0, d->stream>>>(d->stage, d->zbase, R, Cc, d->ntc);
     k_bed_offsets<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, d->zbase, (float*)p, R, Cc, d->ntc);
     TRI_CUDA_TRY(cudaGetLastError());
-    TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));  // 'base' leaves scope
   } else {
     TRI_CUDA_TRY(cudaMemcpyAsync(d->stage, host, n * 8, cudaMemcpyHostToDevice, d->stream));
     k_from_f64<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, (float*)p, n);
+    TRI_CUDA_TRY(cudaGetLastError());
+  }
+  if (field == TRI_FIELD_MAXH) {  // dry bands skip the wet-dry kernel only while no max depth is negative
+    TRI_CUDA_TRY(cudaMemsetAsync(d->maxh_neg, 0, sizeof(int32_t), d->stream));
+    if (d->prec == TRI_FP64)
+      k_flag_negative<double><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const double*)p, n, d->maxh_neg);
+    else
+      k_flag_negative<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const float*)p, n, d->maxh_neg);
     TRI_CUDA_TRY(cudaGetLastError());
   }
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));

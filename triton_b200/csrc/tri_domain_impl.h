@@ -71,7 +71,7 @@ struct tri_domain {
   uint8_t* tzero = nullptr;
   int64_t tz_cap = 0, tz_tiles = 0;
   bool tz_on = false, tz_dirty = true;
-  bool maxh_nonneg = true;  // every max depth uploaded is >= 0
+  int32_t* maxh_neg = nullptr;  // device flag: an uploaded max depth is negative (or NaN)
   std::vector<uint8_t> tz_pin_host;
   double tuned_ms = 0;
   // graphs of 'graph_steps' steps

@@ -1076,12 +1076,12 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_dt(DevClock* __restrict__ c
 
 // True when every flux tile covering this block's band holds only +0 in the
 // step's destination buffer (tzero: the flux kernel's [2][tiles] flags).  A
-// band without a wet cell has nothing to mask, no wave speed, and (with max
-// depths and the arrival depth non-negative, which the host ensures before
-// it passes the flags) no max depth or arrival to record.  Cell (r, c)
-// belongs to tile row max(r-1,0)/rb and strip max(c-1,0)/kStripCols, clamped:
-// ghost rows and columns belong to the edge tiles that copy them.  Uniform
-// over the block.
+// band without a wet cell has nothing to mask and no wave speed, and it
+// records no max depth or arrival while no max depth is negative (a device
+// flag set by max depth uploads) and the arrival depth is not (the host
+// passes no flags then).  Cell (r, c) belongs to tile row max(r-1,0)/rb and
+// strip max(c-1,0)/kStripCols, clamped: ghost rows and columns belong to the
+// edge tiles that copy them.  Uniform over the block.
 template <typename T>
 __device__ __forceinline__ bool band_all_zero(const DevClock* clk, const uint8_t* __restrict__ tzero, int rows,
                                               int cols, int rb, int bx, int by) {
@@ -1102,11 +1102,12 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
                                                             const BedMap<T> bed, T* __restrict__ maxh, int rows,
                                                             int cols, T hextra, float* __restrict__ arrival,
                                                             float arrival_depth, const uint8_t* __restrict__ tzero,
-                                                            int rb) {
+                                                            int rb, const int32_t* __restrict__ maxh_neg) {
   extern __shared__ __align__(128) unsigned char wet_smem[];
   if (!clk->active) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
-  if (tzero != nullptr && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) return;
+  if (tzero != nullptr && *maxh_neg == 0 && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y))
+    return;
   if (threadIdx.x == 0) {  // interior cells of this band
     const int ra = max((int)blockIdx.y * WetStage<T>::kBand, 1);
     const int rz = min((int)blockIdx.y * WetStage<T>::kBand + WetStage<T>::kBand - 1, rows - 2);

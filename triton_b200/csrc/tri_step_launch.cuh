@@ -73,7 +73,8 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + WetStage<T>::kBand - 1) / WetStage<T>::kBand);
   if (ev) cudaEventRecord(ev[2], s);
   k_wetdry_staged<T><<<g2, kWetCols, WetStage<T>::kBytes, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, hx,
-                                                                 a.arrival, a.arrival_depth, a.tzero_wet, a.rb);
+                                                                 a.arrival, a.arrival_depth, a.tzero_wet, a.rb,
+                                                                 a.maxh_neg);
   if (ev) cudaEventRecord(ev[3], s);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;

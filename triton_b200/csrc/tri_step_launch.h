@@ -68,9 +68,11 @@ struct StepArgs {
   float arrival_depth;
   // dry-tile flags of the flux kernel ([2][tiles] by buffer + [tiles]
   // pinned), or null to compute every tile; the same for the wet-dry kernel
-  // (null also while a max depth or the arrival depth is negative)
+  // (null also while the arrival depth is negative), which skips bands only
+  // while *maxh_neg (an uploaded max depth is negative) is 0
   uint8_t* tzero;
   const uint8_t* tzero_wet;
+  const int32_t* maxh_neg;
 };
 
 // One time step (clock, flux/update, sources, open ghosts, boundary cells,
