@@ -6,6 +6,9 @@
   scenario the case was written from, value for value.
 * libtriton_b200.so loads and exports every symbol include/triton_b200.h
   declares.
+* The ASCII raster formatter gives printf's "%.6f" text for every double:
+  exact ties, negatives that round to zero, subnormals, values past its
+  integer range, infinities.
 """
 import os
 import re
@@ -128,3 +131,27 @@ def test_footprint():
     from triton_b200 import Domain
     assert Domain.footprint(8194, 8194, "fp64") > 8194 * 8194 * 72
     assert Domain.footprint(8194, 8194, "fp32") < Domain.footprint(8194, 8194, "fp64")
+
+
+def test_ascii_formatter_matches_printf(tmp_path):
+    rng = np.random.default_rng(5)
+    mag = 10.0 ** rng.uniform(-12, 15, 200000)
+    vals = [mag * rng.choice([-1.0, 1.0], mag.size),
+            (2 * rng.integers(0, 5 * 10 ** 5, 20000) + 1) / 128.0,  # exact decimal ties at the 6th digit
+            -(2 * rng.integers(0, 5 * 10 ** 5, 2000) + 1) / 128.0,
+            rng.integers(-10 ** 9, 10 ** 9, 20000) / 10.0 ** rng.integers(0, 9, 20000),
+            np.array([0.0, -0.0, 5e-7, -5e-7, 4.9999999e-7, -1e-9, 2.0 ** -1074, -(2.0 ** -1074), 2.0 ** -1022,
+                      0.0078125, 0.0234375, 1.0000005, 123456.0000005, 9.9999995, 18446744073709.55,
+                      18446744073709.553, 1.8446744073709552e13, 2.0 ** 64, 1e20, -1e20, 1e300, -1.7976931348623157e308,
+                      np.inf, -np.inf])]
+    v = np.concatenate(vals)
+    src = tmp_path / "v.f64"
+    v.astype("<f8").tofile(src)
+    out = tmp_path / "v.txt"
+    p = subprocess.run([EXE, "--format-fixed6", str(src), str(out)], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    got = out.read_text().splitlines()
+    assert len(got) == v.size
+    want = ["%.6f" % x for x in v]  # Python's formatting is correctly rounded, ties to even, like glibc's
+    bad = [(float(x), g, w) for x, g, w in zip(v, got, want) if g != w]
+    assert not bad, bad[:10]

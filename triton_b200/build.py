@@ -72,7 +72,8 @@ def build(verbose=False):
     if host_srcs:
         hdrs = glob.glob(os.path.join(HOST, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
         if _newer(EXE, host_srcs + hdrs + [LIB]):
-            cmd = ["g++", "-std=c++20", "-O2", "-I" + os.path.join(ROOT, "include"), "-I" + HOST] + host_srcs + \
+            cmd = ["g++", "-std=c++20", "-O2", "-pthread", "-I" + os.path.join(ROOT, "include"), "-I" + HOST] + \
+                host_srcs + \
                 ["-o", EXE, "-L" + LIBDIR, "-ltriton_b200", "-Wl,-rpath,$ORIGIN"]
             if verbose:
                 print(" ".join(cmd))

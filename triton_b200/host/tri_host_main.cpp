@@ -8,15 +8,19 @@
 #include <sys/stat.h>
 #include <sys/time.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <future>
 #include <iomanip>
 #include <iostream>
 #include <limits>
 #include <sstream>
+#include <thread>
 
+#include "tri_fixed6.h"
 #include "tri_host.h"
 #include "triton_b200.h"
 
@@ -65,6 +69,7 @@ struct Timers {
 struct Output {
   const Problem& P;
   std::string root;  // project_dir/output_folder
+  int threads = 1;   // host threads formatting ASCII rasters
   explicit Output(const Problem& p) : P(p), root(p.project_dir + "/" + p.args.output_folder) {}
 
   std::string mat_path(const std::string& what, const std::string& sub, int print_id) const {
@@ -84,24 +89,40 @@ struct Output {
     f.write(reinterpret_cast<const char*>(&hc), sizeof(double));
     for (int i = 1; i < R - 1; i++) f.write(reinterpret_cast<const char*>(&a[(size_t)i * C + 1]), (C - 2) * sizeof(double));
   }
-  // write_output_ascii_sequential (output_ascii.h:12-81): fixed, 6 decimals
+  // write_output_ascii_sequential (output_ascii.h:12-81): fixed, 6 decimals,
+  // one line per interior row.  Bands of rows are formatted on 'threads'
+  // threads (trihost::append_fixed6 gives printf's "%.6f" text) and written
+  // in row order.
   void ascii(const std::vector<double>& a, const std::string& what, int print_id) const {
     ensure_dir(root + "/");
     ensure_dir(root + "/asc/");
     FILE* f = std::fopen(mat_path(what, "asc", print_id).c_str(), "w");
     if (!f) return;
-    const int R = P.rows, C = P.cols;
-    std::string line;
-    char buf[64];
-    for (int i = 1; i < R - 1; i++) {
-      line.clear();
-      for (int j = 1; j < C - 1; j++) {
-        int n = std::snprintf(buf, sizeof(buf), "%.6f", a[(size_t)i * C + j]);
-        line.append(buf, n);
-        if (j < C - 2) line.push_back(' ');
+    const int R = P.rows, C = P.cols, nt = std::max(1, threads);
+    const int band = std::max(1, std::min(256, (R - 2 + nt - 1) / nt));
+    auto format_rows = [&](int i0, int i1, std::string& text) {
+      text.clear();
+      text.reserve((size_t)(i1 - i0) * (size_t)(C - 2) * 10);
+      for (int i = i0; i < i1; i++) {
+        for (int j = 1; j < C - 1; j++) {
+          trihost::append_fixed6(text, a[(size_t)i * C + j]);
+          if (j < C - 2) text.push_back(' ');
+        }
+        text.push_back('\n');
       }
-      line.push_back('\n');
-      std::fwrite(line.data(), 1, line.size(), f);
+    };
+    std::vector<std::string> parts((size_t)nt);
+    for (int r0 = 1; r0 < R - 1; r0 += nt * band) {
+      std::vector<std::thread> pool;
+      for (int t = 0; t < nt; t++) {
+        const int i0 = std::min(R - 1, r0 + t * band), i1 = std::min(R - 1, i0 + band);
+        if (t == nt - 1)
+          format_rows(i0, i1, parts[(size_t)t]);
+        else
+          pool.emplace_back(format_rows, i0, i1, std::ref(parts[(size_t)t]));
+      }
+      for (std::thread& th : pool) th.join();
+      for (const std::string& text : parts) std::fwrite(text.data(), 1, text.size(), f);
     }
     std::fclose(f);
   }
@@ -238,6 +259,9 @@ int run(int argc, char** argv) {
   std::cerr << C_GREEN "[OK] " C_RESET "Simulation starts" << std::endl;
   T.start("simulation");
   Output out(P);
+  // [nthreads] (the reference's OpenMP thread count) formats the ASCII rasters
+  out.threads = argc > 2 ? std::max(1, std::atoi(argv[2]))
+                         : (int)std::max(1u, std::thread::hardware_concurrency());
   double simtime = P.simtime;
   const size_t nobs = P.obs_cells.size();
   std::vector<double> oh(nobs), oqx(nobs), oqy(nobs);
@@ -274,6 +298,17 @@ int run(int argc, char** argv) {
   ok(tri_domain_set_clock(d, &c), "set clock");
   int it_count_average = 0;
   std::vector<double> bh(n), bqx(n), bqy(n), bmh(n);
+  // The rasters of an output time, its restart cfg and cid are written by a
+  // background task while the GPU goes on stepping; the next output time
+  // waits for it before it downloads into the same buffers (the cfg and cid
+  // name a checkpoint only once its rasters are complete).
+  std::future<void> writing;
+  auto finish_writing = [&]() {
+    if (!writing.valid()) return;
+    T.start("io");
+    writing.get();
+    T.stop("io");
+  };
   while (true) {
     T.start("compute");
     tri_progress p{};
@@ -294,25 +329,27 @@ int run(int argc, char** argv) {
     }
     if (p.events & TRI_EV_PRINT) {
       c.print_id++;
+      finish_writing();
       T.start("compute");
       ok(tri_domain_download(d, TRI_FIELD_H, bh.data(), n), "download h");
       ok(tri_domain_download(d, TRI_FIELD_QX, bqx.data(), n), "download qx");
       ok(tri_domain_download(d, TRI_FIELD_QY, bqy.data(), n), "download qy");
       if (!a.max_value_print_option.empty()) ok(tri_domain_download(d, TRI_FIELD_MAXH, bmh.data(), n), "download maxh");
       T.stop("compute");
-      T.start("io");
-      const std::string& po = a.print_option;
-      if (po.find('h') != std::string::npos) out.write("H", bh, c.print_id);
-      if (po.find('u') != std::string::npos) out.write("QX", bqx, c.print_id);
-      if (po.find('v') != std::string::npos) out.write("QY", bqy, c.print_id);
-      if (!a.max_value_print_option.empty() && a.max_value_print_option.find('h') != std::string::npos)
-        out.write("MH", bmh, c.print_id);
-      std::cerr << C_BLUE "[" << c.print_id << "]" C_RESET " File written at time " << simtime << " seconds.\n";
-      out.restart_cfg(simtime, c.print_id, c.average_dt, c.it_count);
-      std::ofstream cid("cid");
-      cid << c.print_id;
-      cid.close();
-      T.stop("io");
+      const int pid = c.print_id, itc = c.it_count;
+      const double t_out = simtime, avg_dt = c.average_dt;
+      writing = std::async(std::launch::async, [&out, &a, &bh, &bqx, &bqy, &bmh, pid, itc, t_out, avg_dt]() {
+        const std::string& po = a.print_option;
+        if (po.find('h') != std::string::npos) out.write("H", bh, pid);
+        if (po.find('u') != std::string::npos) out.write("QX", bqx, pid);
+        if (po.find('v') != std::string::npos) out.write("QY", bqy, pid);
+        if (!a.max_value_print_option.empty() && a.max_value_print_option.find('h') != std::string::npos)
+          out.write("MH", bmh, pid);
+        std::cerr << C_BLUE "[" << pid << "]" C_RESET " File written at time " << t_out << " seconds.\n";
+        out.restart_cfg(t_out, pid, avg_dt, itc);
+        std::ofstream cid("cid");
+        cid << pid;
+      });
       T.stop("simulation");
       T.stop("total");
       out.times(T, c.print_id);
@@ -322,6 +359,7 @@ int run(int argc, char** argv) {
     ok(tri_domain_set_clock(d, &c), "set clock");
     if ((p.events & TRI_EV_END) || (p.steps == 0 && p.events == 0)) break;
   }
+  finish_writing();
   if (a.time_series_flag) observe();
   T.stop("simulation");
   T.stop("total");
@@ -372,9 +410,27 @@ int dump_problem(const char* argv0, const std::string& dir, const std::string& c
   return 0;
 }
 
+// `triton_b200 --format-fixed6 <in.f64> <out.txt>`: the ASCII raster text of
+// raw little-endian doubles, one per line (for tests; no GPU).
+int format_fixed6(const std::string& in, const std::string& outp) {
+  std::ifstream f(in, std::ios::binary);
+  std::vector<char> raw((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  std::string text;
+  for (size_t i = 0; i + 8 <= raw.size(); i += 8) {
+    double v;
+    std::memcpy(&v, raw.data() + i, 8);
+    trihost::append_fixed6(text, v);
+    text.push_back('\n');
+  }
+  std::ofstream o(outp, std::ios::binary);
+  o.write(text.data(), (std::streamsize)text.size());
+  return 0;
+}
+
 int main(int argc, char** argv) {
   try {
     if (argc >= 4 && std::strcmp(argv[1], "--dump-problem") == 0) return dump_problem(argv[0], argv[2], argv[3]);
+    if (argc >= 4 && std::strcmp(argv[1], "--format-fixed6") == 0) return format_fixed6(argv[2], argv[3]);
     return run(argc, argv);
   } catch (const InputError& e) {
     std::cerr << C_RED "[ERROR] " C_RESET << e.what() << std::endl;

@@ -15,6 +15,8 @@ scenario for the same simulated time; the report gives
 """
 from __future__ import annotations
 
+import time
+
 import numpy as np
 
 
@@ -32,6 +34,7 @@ def run_form(sc, precision, duration=None, arrival_depth=0.1, autotune=False, pr
         v0 = d.volume()
         steps = 0
         chunk = 2000 if progress else 1 << 30
+        t0 = time.perf_counter()
         while True:
             n, ev = d.advance(chunk)
             steps += n
@@ -39,7 +42,8 @@ def run_form(sc, precision, duration=None, arrival_depth=0.1, autotune=False, pr
                 print(f"  {precision}: {steps} steps, simtime {d.get_clock().simtime:.1f} s", flush=True)
             if ev & 1 or n == 0:
                 break
-        out = dict(h=d.download("h"), arrival=d.arrival(), volume=d.volume(), v0=v0, steps=steps,
+        wall = time.perf_counter() - t0  # the stepping loop only
+        out = dict(h=d.download("h"), arrival=d.arrival(), volume=d.volume(), v0=v0, steps=steps, wall_s=wall,
                    simtime=d.get_clock().simtime, balance=d.mass_balance())
     finally:
         d.close()
@@ -66,6 +70,7 @@ def compare(sc, duration=None, arrival_depth=0.1, fixed_dt=None):
     dacc = {k: b["balance"][k] - a["balance"][k] for k in terms}
     return dict(
         steps_fp64=a["steps"], steps_fp32=b["steps"], simtime=a["simtime"],
+        wall_fp64_s=a["wall_s"], wall_fp32_s=b["wall_s"],
         max_depth_error_m=float(err.max()), rms_depth_error_m=float(np.sqrt(np.mean(err ** 2))),
         p999_depth_error_m=float(np.quantile(err, 0.999)),
         cells_over_1mm=int((err > 1e-3).sum()), worst_cell=tuple(int(i) + 1 for i in worst),
