@@ -185,6 +185,44 @@ def reference_arm(args, sc, desc):
     print(json.dumps(line))
 
 
+# -- ranks: one process per GPU, replicas of the workload ---------------------
+def ranks():
+    """(rank, world size, local rank) from the torchrun environment."""
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def init_ranks(world, backend="nccl"):
+    """Joins the process group when there is more than one rank (a short
+    timeout, so ranks that wait for a missing one end with an error)."""
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (every rank gets it)."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def close_ranks(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def _timed(stream, fn):
     """Runs fn() between two CUDA events on `stream`; returns (result, ms)."""
     import torch
@@ -307,9 +345,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
+    rank, world, local = ranks()
     if args.workload == "serve":
         if rank == 0:
             serve_arm(args)
@@ -322,18 +358,11 @@ def main():
         return
 
     import torch
-    import torch.distributed as dist
 
     from triton_b200 import Domain  # noqa: F401  (fails loudly if the library is missing)
 
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    init_ranks(world, "nccl")
 
     stream = torch.cuda.current_stream()
     d = sc.to_domain(args.precision, stream=stream.cuda_stream)
@@ -347,7 +376,7 @@ def main():
         tuning = d.autotune(trial_steps=8)
     n, _ = d.advance(args.warmup)
     assert n == args.warmup
-    barrier()
+    barrier(world)
     torch.cuda.synchronize()
     sampler = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ
                            else os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
@@ -357,7 +386,7 @@ def main():
     n, ev = d.advance(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    barrier()
+    barrier(world)
     assert n == args.steps, (n, ev)
     ms = e0.elapsed_time(e1)
     # per-launch durations for the roofline: the same number of steps again
@@ -367,16 +396,13 @@ def main():
     d.set_timing(True)
     n_r, ev = d.advance(args.steps)
     torch.cuda.synchronize()
-    barrier()
+    barrier(world)
     clocks = sampler.stop()
     assert n_r == args.steps, (n_r, ev)
     flux_ms, flux_n, wet_ms, wet_n = d.get_timing()
     flux_cells, wet_cells = d.get_work()  # interior cells the launches computed (dry tiles skipped)
     d.set_timing(False)
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, "cuda")
     cells = sc.interior_cells
     value = cells * args.steps * world / (ms_max / 1000.0)
 
@@ -394,7 +420,7 @@ def main():
     from triton_b200 import _abi
     L = _abi.lib()
     fid = {"h": 0, "qx": 1, "qy": 2, "n2": 3, "z": 4, "maxh": 5}
-    barrier()
+    barrier(world)
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
@@ -406,12 +432,9 @@ def main():
         _abi.check(L.tri_domain_download(d2._h, fid[k], C.cast(outs[k].data_ptr(), _abi._dp), sc.rows * sc.cols))
     f1.record(stream)
     torch.cuda.synchronize()
-    barrier()
+    barrier(world)
     ems = f0.elapsed_time(f1)
-    te = torch.tensor([ems], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_val = cells * n2_ * world / (float(te.item()) / 1000.0)
+    e2e_val = cells * n2_ * world / (max_over_ranks(ems, world, "cuda") / 1000.0)
     h2d = 6 * sc.rows * sc.cols * 8
     d2h = 4 * sc.rows * sc.cols * 8
     d2.close()
@@ -473,8 +496,7 @@ def main():
             line["forms"] = forms
         print(json.dumps(line))
     d.close()
-    if world > 1:
-        dist.destroy_process_group()
+    close_ranks(world)
 
 
 if __name__ == "__main__":
