@@ -221,6 +221,13 @@ struct FluxCtx {
   int nroff, roff_rows, roff_row;
   uint32_t step;  // it_count of the running step (seeds the FP32 form's rounding of runoff)
   StepK<T> K;
+  // Dry-tile skipping (null: every tile is computed).  tz_src[t] / tz_dst[t]:
+  // tile t of the source / destination buffer holds only zero bits in h, qx
+  // and qy; tpin[t]: tile t is never skipped (a later kernel of the step
+  // writes into it: sources, external boundary cells, open boundaries).
+  const uint8_t* tz_src;
+  uint8_t* tz_dst;
+  const uint8_t* tpin;
 };
 
 template <typename T>
@@ -253,6 +260,9 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   X.K.rdx = rdx;
   X.K.rdt = T(clk->rdt);
   X.K.hextra = hextra;
+  X.tz_src = nullptr;
+  X.tz_dst = nullptr;
+  X.tpin = nullptr;
   return X;
 }
 
@@ -261,31 +271,27 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
 __device__ __forceinline__ bool nonzero_bits(double v) { return __double_as_longlong(v) != 0; }
 __device__ __forceinline__ bool nonzero_bits(float v) { return __float_as_uint(v) != 0u; }
 
-// Dry-tile flags of the flux kernel: tzero = [2][ntiles] bytes, byte t of
-// buffer b set when tile t holds only zero bits in h, qx and qy of state
-// buffer b, then [ntiles] pinned bytes (tiles never skipped: a later kernel of
-// the step writes into them: sources, external boundary cells, open
-// boundaries).  A tile whose cells and whose four neighbour tiles' cells hold
-// only +0 in the source buffer computes exactly +0 everywhere (every face is
-// dry-dry and contributes nothing; no runoff on such a domain), and if its
-// cells in the destination buffer hold +0 already (it was all-zero two steps
-// ago), it has nothing to write.
-__device__ __forceinline__ bool tile_skippable(const uint8_t* __restrict__ tzero, size_t ntiles, int src, int dst,
-                                               unsigned tile, int ns, int nty) {
-  const uint8_t* zs = tzero + (size_t)src * ntiles;
+// A tile whose cells and whose four neighbour tiles' cells hold only +0 in
+// the source buffer computes exactly +0 everywhere (every face is dry-dry and
+// contributes nothing; no runoff on such a domain), and if its cells in the
+// destination buffer hold +0 already (it was all-zero two steps ago), it has
+// nothing to write.  Only lane 0's answer counts.
+template <typename T>
+__device__ __forceinline__ bool tile_skippable(const FluxCtx<T>& X, unsigned tile) {
+  if (X.tz_src == nullptr) return false;
+  const int ns = X.nstrips, nty = (X.rows - 2 + X.rb - 1) / X.rb;
   const int sx = (int)(tile % ns), ry = (int)(tile / ns);
-  if (!(zs[tile] & tzero[(size_t)dst * ntiles + tile]) || tzero[2 * ntiles + tile]) return false;
-  if (sx > 0 && !zs[tile - 1]) return false;
-  if (sx < ns - 1 && !zs[tile + 1]) return false;
-  if (ry > 0 && !zs[tile - ns]) return false;
-  if (ry < nty - 1 && !zs[tile + ns]) return false;
+  if (!(X.tz_src[tile] & X.tz_dst[tile]) || X.tpin[tile]) return false;
+  if (sx > 0 && !X.tz_src[tile - 1]) return false;
+  if (sx < ns - 1 && !X.tz_src[tile + 1]) return false;
+  if (ry > 0 && !X.tz_src[tile - ns]) return false;
+  if (ry < nty - 1 && !X.tz_src[tile + ns]) return false;
   return true;
 }
 
-// One warp tile: strip sx (30 interior columns), rows r0..r1.  Returns, on
-// every lane, whether any lane wrote a value other than +0.
+// One warp tile: strip sx (30 interior columns), rows r0..r1.
 template <typename T>
-__device__ __forceinline__ bool flux_tile(const FluxCtx<T>& X, unsigned tile, int lane) {
+__device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, int lane) {
   const int rows = X.rows, cols = X.cols, rb = X.rb;
   const T dt = X.K.dt, hextra = X.K.hextra;
   const T* __restrict__ hi = X.hi;
@@ -431,7 +437,10 @@ __device__ __forceinline__ bool flux_tile(const FluxCtx<T>& X, unsigned tile, in
       if (acc_c != 0.0) atomicAdd(&X.clk->acc_step[kAccClip], acc_c);
     }
   }
-  return __any_sync(0xffffffffu, wrote_nonzero);
+  if (X.tz_dst != nullptr) {
+    const bool nz = __any_sync(0xffffffffu, wrote_nonzero);
+    if (lane == 0) X.tz_dst[tile] = (!nz && !X.tpin[tile]) ? 1 : 0;
+  }
 }
 
 template <typename T, int MINB>
@@ -441,30 +450,32 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
                                                      int rows, int cols, int rb, T dx, T rdx, T hextra,
                                                      uint8_t* __restrict__ tzero) {
   if (!clk->active) return;
-  const FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
+  FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
   const int lane = threadIdx.x & 31;
-  const int ns = X.nstrips, nty = (rows - 2 + rb - 1) / rb;
-  const unsigned ntiles = (unsigned)ns * (unsigned)nty;
-  unsigned work = 0;  // interior cells of the tiles this warp computed (lane 0; < 2^31 cells per grid)
+  const unsigned ntiles = (unsigned)X.nstrips * (unsigned)((rows - 2 + rb - 1) / rb);
+  if (tzero != nullptr) {  // [2][ntiles] zero flags by buffer, then [ntiles] pinned
+    X.tz_src = tzero + (size_t)clk->src * ntiles;
+    X.tz_dst = tzero + (size_t)clk->dst * ntiles;
+    X.tpin = tzero + 2 * (size_t)ntiles;
+  }
+  unsigned long long work = 0;  // interior cells of the tiles this warp computed (lane 0)
   while (true) {
     unsigned tile = 0;
     int skip = 0;
     if (lane == 0) {
       tile = atomicAdd(&clk->tile_next, 1u);
-      skip = tile < ntiles && tzero != nullptr && tile_skippable(tzero, ntiles, clk->src, clk->dst, tile, ns, nty);
+      skip = tile < ntiles && tile_skippable<T>(X, tile);
       if (tile < ntiles && !skip) {
-        const int sx = (int)(tile % ns), r0 = 1 + (int)(tile / ns) * rb;
-        work += (unsigned)((min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols));
+        const int sx = (int)(tile % X.nstrips), r0 = 1 + (int)(tile / X.nstrips) * rb;
+        work += (unsigned long long)(min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols);
       }
     }
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
     if (__shfl_sync(0xffffffffu, skip, 0)) continue;
-    const bool nz = flux_tile<T>(X, tile, lane);
-    if (tzero != nullptr && lane == 0)  // this tile of the destination buffer: only +0 now?
-      tzero[(size_t)clk->dst * ntiles + tile] = (!nz && !tzero[2 * (size_t)ntiles + tile]) ? 1 : 0;
+    flux_tile<T>(X, tile, lane);
   }
-  if (lane == 0 && work) atomicAdd(&clk->work_flux, (unsigned long long)work);
+  if (lane == 0 && work) atomicAdd(&clk->work_flux, work);
 }
 
 // ---------------------------------------------------------------------------
