@@ -182,11 +182,11 @@ int tri_domain_download_arrival(tri_domain* d, double* host, int64_t n);
 int tri_domain_set_timing(tri_domain* d, int32_t enabled);
 int tri_domain_get_timing(tri_domain* d, double* flux_ms, int32_t* flux_launches, double* wetdry_ms,
                           int32_t* wetdry_launches);
-/* Interior cells of the flux tiles and wet-dry bands that single-domain
- * advance() calls computed since the last tri_domain_set_timing: tiles whose
- * cells and neighbours hold only zeros are skipped (their update is exactly
- * the identity) and not counted.  No reference counterpart (the reference
- * updates every cell every step). */
+/* Interior cells of the flux tiles and wet-dry bands that advance() calls
+ * computed since the last tri_domain_set_timing (steps run x interior cells,
+ * less the cells of tiles skipped as dry: tiles whose cells and neighbours
+ * hold only zeros, whose update is exactly the identity).  No reference
+ * counterpart (the reference updates every cell every step). */
 int tri_domain_get_work(tri_domain* d, int64_t* flux_cells, int64_t* wetdry_cells);
 
 /* Launch-shape autotuner of the flux kernel.  Runs trial_steps steps of the

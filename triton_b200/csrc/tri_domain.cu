@@ -863,6 +863,7 @@ int tri_domain_advance(tri_domain* d, int32_t max_steps, tri_progress* p) {
   if (rc != TRI_OK) return rc;
   p->steps = m->steps;
   p->events = m->events;
+  d->work_steps += m->steps;
   if (m->status != 0)
     return set_error(TRI_E_TIMEOUT, "a device-side wait gave up during the last advance (status %d); the state "
                      "of this domain is not valid", m->status);
@@ -1072,15 +1073,20 @@ int tri_domain_set_timing(tri_domain* d, int32_t enabled) {
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
   d->timing = enabled != 0;
   d->tev_used = 0;
-  d->mirror->work_flux = d->mirror->work_wet = 0;  // sent with the clock at the next advance
+  memset(d->mirror->skipped, 0, sizeof(d->mirror->skipped));  // sent with the clock at the next advance
+  d->work_steps = 0;
   return TRI_OK;
 }
 
 int tri_domain_get_work(tri_domain* d, int64_t* flux_cells, int64_t* wetdry_cells) {
   TRI_CHECK_ARG(d, "null domain");
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
-  if (flux_cells) *flux_cells = (int64_t)d->mirror->work_flux;
-  if (wetdry_cells) *wetdry_cells = (int64_t)d->mirror->work_wet;
+  const int64_t all = d->work_steps * (int64_t)(d->desc.rows - 2) * (d->desc.cols - 2);
+  int64_t sk[2] = {0, 0};
+  for (int k = 0; k < 2; k++)
+    for (int i = 0; i < kSkipSlots; i++) sk[k] += (int64_t)d->mirror->skipped[k][i];
+  if (flux_cells) *flux_cells = all - sk[0];
+  if (wetdry_cells) *wetdry_cells = all - sk[1];
   return TRI_OK;
 }
 

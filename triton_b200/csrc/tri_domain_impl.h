@@ -72,6 +72,7 @@ struct tri_domain {
   int64_t tz_cap = 0, tz_tiles = 0;
   bool tz_on = false, tz_dirty = true;
   int32_t* maxh_neg = nullptr;  // device flag: an uploaded max depth is negative (or NaN)
+  int64_t work_steps = 0;       // steps advance() ran since tri_domain_set_timing
   std::vector<uint8_t> tz_pin_host;
   double tuned_ms = 0;
   // graphs of 'graph_steps' steps

@@ -289,8 +289,10 @@ __device__ __forceinline__ bool tile_skippable(const FluxCtx<T>& X, unsigned til
   return true;
 }
 
-// One warp tile: strip sx (30 interior columns), rows r0..r1.
-template <typename T>
+// One warp tile: strip sx (30 interior columns), rows r0..r1.  kTrack:
+// record in X.tz_dst whether the tile wrote only +0 (dry-tile skipping; the
+// kernels of domains that cannot skip are built without it).
+template <typename T, bool kTrack>
 __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, int lane) {
   const int rows = X.rows, cols = X.cols, rb = X.rb;
   const T dt = X.K.dt, hextra = X.K.hextra;
@@ -316,11 +318,17 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   bool wrote_nonzero = false;  // any value this lane writes is not +0
   auto copy_ghost = [&](int r) {
     const size_t id = (size_t)r * cols + c;
-    const T gh = hi[id], gqx = qxi[id], gqy = qyi[id];
-    ho[id] = gh;
-    qxo[id] = gqx;
-    qyo[id] = gqy;
-    wrote_nonzero |= nonzero_bits(gh) | nonzero_bits(gqx) | nonzero_bits(gqy);
+    if (kTrack) {
+      const T gh = hi[id], gqx = qxi[id], gqy = qyi[id];
+      ho[id] = gh;
+      qxo[id] = gqx;
+      qyo[id] = gqy;
+      wrote_nonzero |= nonzero_bits(gh) | nonzero_bits(gqx) | nonzero_bits(gqy);
+    } else {
+      ho[id] = hi[id];
+      qxo[id] = qxi[id];
+      qyo[id] = qyi[id];
+    }
   };
 
   // raw values of the next row are loaded one iteration ahead
@@ -395,7 +403,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       ho[id] = hn;
       qxo[id] = qn;
       qyo[id] = vn;
-      wrote_nonzero |= nonzero_bits(hn) | nonzero_bits(qn) | nonzero_bits(vn);
+      if (kTrack) wrote_nonzero |= nonzero_bits(hn) | nonzero_bits(qn) | nonzero_bits(vn);
     }
     if (r > r1) {
       if (r == rows - 1 && owner) copy_ghost(r);
@@ -437,13 +445,14 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       if (acc_c != 0.0) atomicAdd(&X.clk->acc_step[kAccClip], acc_c);
     }
   }
-  if (X.tz_dst != nullptr) {
+  if (kTrack) {
     const bool nz = __any_sync(0xffffffffu, wrote_nonzero);
     if (lane == 0) X.tz_dst[tile] = (!nz && !X.tpin[tile]) ? 1 : 0;
   }
 }
 
-template <typename T, int MINB>
+// kSkip: the domain keeps dry-tile flags (tzero) and skips dry tiles.
+template <typename T, int MINB, bool kSkip>
 __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict__ clk, StateBufs<T> sb,
                                                      const BedMap<T> bed, const T* __restrict__ n2,
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
@@ -453,29 +462,30 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
   FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
   const int lane = threadIdx.x & 31;
   const unsigned ntiles = (unsigned)X.nstrips * (unsigned)((rows - 2 + rb - 1) / rb);
-  if (tzero != nullptr) {  // [2][ntiles] zero flags by buffer, then [ntiles] pinned
+  if (kSkip) {  // [2][ntiles] zero flags by buffer, then [ntiles] pinned
     X.tz_src = tzero + (size_t)clk->src * ntiles;
     X.tz_dst = tzero + (size_t)clk->dst * ntiles;
     X.tpin = tzero + 2 * (size_t)ntiles;
   }
-  unsigned long long work = 0;  // interior cells of the tiles this warp computed (lane 0)
+  unsigned skipped = 0;  // interior cells of the tiles this warp skipped (lane 0)
   while (true) {
     unsigned tile = 0;
     int skip = 0;
     if (lane == 0) {
       tile = atomicAdd(&clk->tile_next, 1u);
-      skip = tile < ntiles && tile_skippable<T>(X, tile);
-      if (tile < ntiles && !skip) {
+      skip = kSkip && tile < ntiles && tile_skippable<T>(X, tile);
+      if (kSkip && skip) {
         const int sx = (int)(tile % X.nstrips), r0 = 1 + (int)(tile / X.nstrips) * rb;
-        work += (unsigned long long)(min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols);
+        skipped += (unsigned)((min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols));
       }
     }
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if (tile >= ntiles) break;
-    if (__shfl_sync(0xffffffffu, skip, 0)) continue;
-    flux_tile<T>(X, tile, lane);
+    if (kSkip && __shfl_sync(0xffffffffu, skip, 0)) continue;
+    flux_tile<T, kSkip>(X, tile, lane);
   }
-  if (lane == 0 && work) atomicAdd(&clk->work_flux, work);
+  if (kSkip && lane == 0 && skipped)  // spread over the slots: one address would serialize the atomics
+    atomicAdd(&clk->skipped[0][(blockIdx.x * 4 + (threadIdx.x >> 5)) % kSkipSlots], (unsigned long long)skipped);
 }
 
 // ---------------------------------------------------------------------------
@@ -1106,13 +1116,16 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
   extern __shared__ __align__(128) unsigned char wet_smem[];
   if (!clk->active) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
-  if (tzero != nullptr && *maxh_neg == 0 && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y))
+  if (tzero != nullptr && *maxh_neg == 0 && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) {
+    if (threadIdx.x == 0) {  // interior cells of the skipped band
+      const int ra = max((int)blockIdx.y * WetStage<T>::kBand, 1);
+      const int rz = min((int)blockIdx.y * WetStage<T>::kBand + WetStage<T>::kBand - 1, rows - 2);
+      const int ca = max((int)blockIdx.x * kWetCols, 1), cz = min((int)blockIdx.x * kWetCols + kWetCols - 1, cols - 2);
+      if (rz >= ra && cz >= ca)
+        atomicAdd(&clk->skipped[1][(blockIdx.x + blockIdx.y * 7) % kSkipSlots],
+                  (unsigned long long)(rz - ra + 1) * (cz - ca + 1));
+    }
     return;
-  if (threadIdx.x == 0) {  // interior cells of this band
-    const int ra = max((int)blockIdx.y * WetStage<T>::kBand, 1);
-    const int rz = min((int)blockIdx.y * WetStage<T>::kBand + WetStage<T>::kBand - 1, rows - 2);
-    const int ca = max((int)blockIdx.x * kWetCols, 1), cz = min((int)blockIdx.x * kWetCols + kWetCols - 1, cols - 2);
-    if (rz >= ra && cz >= ca) atomicAdd(&clk->work_wet, (unsigned long long)(rz - ra + 1) * (cz - ca + 1));
   }
   const unsigned long long key = wetdry_staged<T>(clk, sb, bed, maxh, rows, cols, hextra, arrival, arrival_depth,
                                                   blockIdx.x, blockIdx.y, reinterpret_cast<T*>(wet_smem));
@@ -1147,7 +1160,7 @@ __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __
     if (!M.clk->active) continue;
     const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
                                      M.hextra);
-    flux_tile<T>(X, tile - M.tile_begin, lane);
+    flux_tile<T, false>(X, tile - M.tile_begin, lane);
   }
 }
 

@@ -33,9 +33,9 @@ StateBufs<T> bufs_of(const StepArgs& a) {
 template <typename T>
 void flux_occupancy(int variant, int* per_sm) {
   switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v0>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v1>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v2>, 128, 0); break;
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v0, false>, 128, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v1, false>, 128, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v2, false>, 128, 0); break;
   }
 }
 
@@ -48,10 +48,18 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   k_clock<<<1, 32, 0, s>>>(a.clk);
   if (ev) cudaEventRecord(ev[0], s);
 #define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero
-  switch (a.flux_variant) {
-    case 0: k_flux_update<T, FluxBudget<T>::v0><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-    case 1: k_flux_update<T, FluxBudget<T>::v1><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-    default: k_flux_update<T, FluxBudget<T>::v2><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+  if (a.tzero != nullptr) {  // dry-tile skipping
+    switch (a.flux_variant) {
+      case 0: k_flux_update<T, FluxBudget<T>::v0, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      case 1: k_flux_update<T, FluxBudget<T>::v1, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      default: k_flux_update<T, FluxBudget<T>::v2, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    }
+  } else {
+    switch (a.flux_variant) {
+      case 0: k_flux_update<T, FluxBudget<T>::v0, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      case 1: k_flux_update<T, FluxBudget<T>::v1, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      default: k_flux_update<T, FluxBudget<T>::v2, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+    }
   }
 #undef TRI_FLUX_ARGS
   if (ev) cudaEventRecord(ev[1], s);

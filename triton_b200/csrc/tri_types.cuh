@@ -17,6 +17,9 @@ constexpr size_t kFieldPad = 256;
 constexpr int kAccTerms = 5;
 enum { kAccBoundary = 0, kAccSources = 1, kAccRunoff = 2, kAccExtbc = 3, kAccClip = 4 };
 
+// Slots of the skipped-cell counters in DevClock.
+constexpr int kSkipSlots = 32;
+
 // Device-resident loop state.  Host mirror: tri_clock plus the bookkeeping
 // fields below.
 struct DevClock {
@@ -42,9 +45,10 @@ struct DevClock {
   double acc_step[kAccTerms];
   double acc_sum[kAccTerms];
   double acc_comp[kAccTerms];
-  // interior cells of the flux tiles and wet-dry bands single-domain steps
-  // computed (dry tiles they skipped are not counted)
-  unsigned long long work_flux, work_wet;
+  // interior cells of the flux tiles [0] and wet-dry bands [1] that dry-tile
+  // skipping left out, summed over slots (one address would serialize the
+  // atomics of a launch)
+  unsigned long long skipped[2][kSkipSlots];
 };
 
 template <typename T>
