@@ -319,9 +319,11 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   auto copy_ghost = [&](int r) {
     const size_t id = (size_t)r * cols + c;
     if (kTrack) {
-      const T gh = hi[id], gqx = qxi[id], gqy = qyi[id];
+      const T gh = hi[id];
       ho[id] = gh;
+      const T gqx = qxi[id];
       qxo[id] = gqx;
+      const T gqy = qyi[id];
       qyo[id] = gqy;
       wrote_nonzero |= nonzero_bits(gh) | nonzero_bits(gqx) | nonzero_bits(gqy);
     } else {
@@ -469,19 +471,18 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
   }
   unsigned skipped = 0;  // interior cells of the tiles this warp skipped (lane 0)
   while (true) {
-    unsigned tile = 0;
-    int skip = 0;
+    unsigned tile = 0;  // lane 0 takes the next tile; bit 31: skip it (tiles < 2^31)
     if (lane == 0) {
       tile = atomicAdd(&clk->tile_next, 1u);
-      skip = kSkip && tile < ntiles && tile_skippable<T>(X, tile);
-      if (kSkip && skip) {
+      if (kSkip && tile < ntiles && tile_skippable<T>(X, tile)) {
         const int sx = (int)(tile % X.nstrips), r0 = 1 + (int)(tile / X.nstrips) * rb;
         skipped += (unsigned)((min(r0 + rb - 1, rows - 2) - r0 + 1) * min(kStripCols, cols - 2 - sx * kStripCols));
+        tile |= 0x80000000u;
       }
     }
     tile = __shfl_sync(0xffffffffu, tile, 0);
-    if (tile >= ntiles) break;
-    if (kSkip && __shfl_sync(0xffffffffu, skip, 0)) continue;
+    if ((tile & 0x7FFFFFFFu) >= ntiles) break;
+    if (kSkip && (tile >> 31)) continue;
     flux_tile<T, kSkip>(X, tile, lane);
   }
   if (kSkip && lane == 0 && skipped)  // spread over the slots: one address would serialize the atomics
