@@ -88,6 +88,16 @@ __device__ __forceinline__ double div_shared(double a, double b, double y) {
 // FP32 form: one multiplication (within 1.5 ulp).
 __device__ __forceinline__ float div_shared(float a, float, float y) { return a * y; }
 
+// Programmatic dependent launch: the step kernels are launched so that the
+// next one may be scheduled while the previous one drains.  Each of them
+// first waits until its predecessor has completed and its memory is visible
+// (pdl_wait, before it reads or writes anything), so the order of their
+// effects is exactly stream order; pdl_trigger lets the successor's launch
+// begin once every block of this grid has reached it.  Both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Integer mix of a cell index and a step number (deterministic, so a batch
 // member rounds exactly as its solo run).
 __device__ __forceinline__ uint32_t cell_hash(uint32_t id, uint32_t step) {

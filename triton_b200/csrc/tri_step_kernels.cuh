@@ -104,6 +104,8 @@ __device__ __forceinline__ bool clock_step(DevClock* __restrict__ c) {
 }
 
 static __global__ void k_clock(DevClock* __restrict__ c) {
+  pdl_wait();
+  pdl_trigger();
   if (threadIdx.x == 0) clock_step(c);
 }
 
@@ -460,6 +462,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
                                                      const int32_t* __restrict__ zone, const T* __restrict__ rates,
                                                      int rows, int cols, int rb, T dx, T rdx, T hextra,
                                                      uint8_t* __restrict__ tzero) {
+  pdl_wait();
   if (!clk->active) return;
   FluxCtx<T> X = flux_ctx<T>(clk, sb, bed, n2, zone, rates, rows, cols, rb, dx, rdx, hextra);
   const int lane = threadIdx.x & 31;
@@ -485,6 +488,7 @@ __global__ void __launch_bounds__(128, MINB) k_flux_update(DevClock* __restrict_
     if (kSkip && (tile >> 31)) continue;
     flux_tile<T, kSkip>(X, tile, lane);
   }
+  pdl_trigger();  // no tile left for this warp
   if (kSkip && lane == 0 && skipped)  // spread over the slots: one address would serialize the atomics
     atomicAdd(&clk->skipped[0][(blockIdx.x * 4 + (threadIdx.x >> 5)) % kSkipSlots], (unsigned long long)skipped);
 }
@@ -498,6 +502,8 @@ template <typename T>
 __global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int32_t* __restrict__ order,
                           int count, int nsrc, const int32_t* __restrict__ cells, const double* __restrict__ hyg_t,
                           const T* __restrict__ hyg_v, T dx) {
+  pdl_wait();
+  pdl_trigger();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count || !clk->active) return;
   const int id = order[k];
@@ -526,6 +532,8 @@ __global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int
 
 template <typename T>
 __global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows, int cols) {
+  pdl_wait();
+  pdl_trigger();
   if (!clk->active) return;
   const int d = clk->dst;
   T* h = sb.H(d);
@@ -689,6 +697,8 @@ __global__ void k_extbc(DevClock* __restrict__ clk, StateBufs<T> sb, const BedMa
                         const int32_t* __restrict__ types, const int32_t* __restrict__ start,
                         const int32_t* __restrict__ nrowsv, const T* __restrict__ var1, const T* __restrict__ var2,
                         int rows, int cols) {
+  pdl_wait();
+  pdl_trigger();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count || !clk->active) return;
   extbc_apply<T>(clk, sb, bed, n2, order[k], cells, types, start, nrowsv, var1, var2, rows, cols);
@@ -1115,6 +1125,8 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
                                                             float arrival_depth, const uint8_t* __restrict__ tzero,
                                                             int rb, const int32_t* __restrict__ maxh_neg) {
   extern __shared__ __align__(128) unsigned char wet_smem[];
+  pdl_wait();
+  pdl_trigger();
   if (!clk->active) return;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
   if (tzero != nullptr && *maxh_neg == 0 && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) {

@@ -39,50 +39,70 @@ void flux_occupancy(int variant, int* per_sm) {
   }
 }
 
+// Launches kernel k after the previous work on stream s with programmatic
+// stream serialization: its blocks may be scheduled while the previous
+// kernel drains; the kernel waits for it (pdl_wait) before touching memory.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 template <typename T>
 int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   const int rows = a.rows, cols = a.cols;
   const T dx = (T)a.dx, hx = (T)a.hextra, rdx = (T)(1.0 / a.dx);
   StateBufs<T> sb = bufs_of<T>(a);
   const BedMap<T> bed = bed_of<T>(a);
-  k_clock<<<1, 32, 0, s>>>(a.clk);
+  TRI_CUDA_TRY(launch_pdl(k_clock, 1, 32, 0, s, a.clk));
   if (ev) cudaEventRecord(ev[0], s);
 #define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero
+#define TRI_FLUX(V, SKIP) TRI_CUDA_TRY(launch_pdl(k_flux_update<T, FluxBudget<T>::V, SKIP>, a.flux_blocks, 128, 0, s, \
+                                                 TRI_FLUX_ARGS))
   if (a.tzero != nullptr) {  // dry-tile skipping
     switch (a.flux_variant) {
-      case 0: k_flux_update<T, FluxBudget<T>::v0, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-      case 1: k_flux_update<T, FluxBudget<T>::v1, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-      default: k_flux_update<T, FluxBudget<T>::v2, true><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      case 0: TRI_FLUX(v0, true); break;
+      case 1: TRI_FLUX(v1, true); break;
+      default: TRI_FLUX(v2, true); break;
     }
   } else {
     switch (a.flux_variant) {
-      case 0: k_flux_update<T, FluxBudget<T>::v0, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-      case 1: k_flux_update<T, FluxBudget<T>::v1, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
-      default: k_flux_update<T, FluxBudget<T>::v2, false><<<a.flux_blocks, 128, 0, s>>>(TRI_FLUX_ARGS); break;
+      case 0: TRI_FLUX(v0, false); break;
+      case 1: TRI_FLUX(v1, false); break;
+      default: TRI_FLUX(v2, false); break;
     }
   }
+#undef TRI_FLUX
 #undef TRI_FLUX_ARGS
   if (ev) cudaEventRecord(ev[1], s);
   for (int w = 0; a.nsrc > 0 && w < a.n_src_waves; w++) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
-    k_sources<T><<<(cnt + 127) / 128, 128, 0, s>>>(a.clk, sb, a.src_order + off, cnt, a.nsrc, a.src_cells, a.hyg_t,
-                                                   (const T*)a.hyg_v, dx);
+    TRI_CUDA_TRY(launch_pdl(k_sources<T>, (cnt + 127) / 128, 128, 0, s, a.clk, sb, a.src_order + off, cnt, a.nsrc,
+                            a.src_cells, a.hyg_t, (const T*)a.hyg_v, dx));
   }
   if (a.open_boundaries) {
     const int n = std::max(rows, cols);
-    k_open_bc<T><<<(n + 255) / 256, 256, 0, s>>>(a.clk, sb, rows, cols);
+    TRI_CUDA_TRY(launch_pdl(k_open_bc<T>, (n + 255) / 256, 256, 0, s, a.clk, sb, rows, cols));
   }
   for (int w = 0; a.nbc > 0 && w < a.n_bc_waves; w++) {
     const int off = a.bc_waves[w], cnt = a.bc_waves[w + 1] - off;
-    k_extbc<T><<<(cnt + 127) / 128, 128, 0, s>>>(a.clk, sb, bed, (const T*)a.n2, a.bc_order + off, cnt, a.bc_cells,
-                                                 a.bc_types, a.bc_start, a.bc_nrows, (const T*)a.bc_v1,
-                                                 (const T*)a.bc_v2, rows, cols);
+    TRI_CUDA_TRY(launch_pdl(k_extbc<T>, (cnt + 127) / 128, 128, 0, s, a.clk, sb, bed, (const T*)a.n2,
+                            a.bc_order + off, cnt, a.bc_cells, a.bc_types, a.bc_start, a.bc_nrows, (const T*)a.bc_v1,
+                            (const T*)a.bc_v2, rows, cols));
   }
   dim3 g2((cols + kWetCols - 1) / kWetCols, (rows + WetStage<T>::kBand - 1) / WetStage<T>::kBand);
   if (ev) cudaEventRecord(ev[2], s);
-  k_wetdry_staged<T><<<g2, kWetCols, WetStage<T>::kBytes, s>>>(a.clk, sb, bed, (T*)a.maxh, rows, cols, hx,
-                                                                 a.arrival, a.arrival_depth, a.tzero_wet, a.rb,
-                                                                 a.maxh_neg);
+  TRI_CUDA_TRY(launch_pdl(k_wetdry_staged<T>, g2, kWetCols, WetStage<T>::kBytes, s, a.clk, sb, bed, (T*)a.maxh,
+                          rows, cols, hx, a.arrival, a.arrival_depth, a.tzero_wet, a.rb, a.maxh_neg));
   if (ev) cudaEventRecord(ev[3], s);
   TRI_CUDA_TRY(cudaGetLastError());
   return TRI_OK;
