@@ -313,8 +313,10 @@ void size_flux_grid(tri_domain* d) {
   d->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
 }
 
-// Default shape before any tuning: the largest tile height that still gives
-// every warp of a full wave about eight tiles.
+// Default shape before any tuning: the middle register budget (variant 1,
+// the fastest of the three on watersheds of 1024^2 to 8192^2) and the
+// largest tile height, 32 down to 8, that still gives every warp of a full
+// wave about eight tiles.
 void choose_shape(tri_domain* d) {
   const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
   int sms = 148, dev = 0;
@@ -322,7 +324,8 @@ void choose_shape(tri_domain* d) {
   const int64_t strips = (cols + kStripCols - 1) / kStripCols;
   const int64_t warps = (int64_t)sms * 12;
   int rb = 32;
-  while (rb > 4 && strips * ((rows + rb - 1) / rb) < 8 * warps) rb /= 2;
+  while (rb > 8 && strips * ((rows + rb - 1) / rb) < 8 * warps) rb /= 2;
+  d->flux_variant = 1;
   d->rb = rb;
   size_flux_grid(d);
 }

@@ -63,7 +63,7 @@ struct tri_domain {
   double* vol_out = nullptr;
   int vol_blocks = 0;
   // launch shape of the flux kernel (tile height, register variant, grid)
-  int rb = 16, flux_blocks = 1, flux_variant = 0;
+  int rb = 16, flux_blocks = 1, flux_variant = 1;
   // dry-tile flags of the flux kernel for the current tile shape: [2][tiles]
   // (tile holds only +0 in buffer 0 / 1) then [tiles] pinned.  Any change of
   // state, forcing or shape outside the step kernels marks them dirty; they

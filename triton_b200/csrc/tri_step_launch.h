@@ -13,21 +13,25 @@
 namespace tri {
 
 constexpr int kStripCols = 30;   // interior columns per warp tile of the flux kernel
-constexpr int kFluxVariants = 3; // register budgets: >= 3, 4, 5 blocks of 128 threads per SM
+constexpr int kFluxVariants = 3; // register budgets (FluxBudget)
 constexpr int kWetCols = 128;    // columns per block of the wet-dry/dt kernel
 constexpr int kWetBand = 16;     // rows per block of the initial-dt kernel
 // Blocks per SM that the flux kernel's three register-budget variants are
-// compiled for (__launch_bounds__ minimum): FP64 needs about 128-150
-// registers a thread, the FP32 form 64-100.
+// compiled for (__launch_bounds__ minimum).  FP64: 124, 96 and 80 registers a
+// thread (the last two spill a little to L1); FP32: 88, 64 and 48.  The
+// kernel is latency bound, so occupancy pays for the spills up to the middle
+// variant on single domains (8192^2 watershed, FP64: 4.57 ms a step with 5
+// blocks against 5.64 with 3); batches of small members run best on the
+// first (FP32: 22.2 G cell-updates/s with 5 blocks against 20.2 with 6).
 template <typename T>
 struct FluxBudget;
 template <>
 struct FluxBudget<double> {
-  static constexpr int v0 = 3, v1 = 4, v2 = 5;
+  static constexpr int v0 = 4, v1 = 5, v2 = 6;
 };
 template <>
 struct FluxBudget<float> {
-  static constexpr int v0 = 5, v1 = 6, v2 = 8;
+  static constexpr int v0 = 5, v1 = 8, v2 = 10;
 };
 // rows per block of the staged wet-dry/dt kernel (its shared-memory tile),
 // and output rows per group of its copies (each group on its own mbarrier)

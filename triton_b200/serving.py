@@ -32,7 +32,7 @@ from .batch import Batch
 from .domain import Domain
 
 # Default launch shapes of the batched flux kernel (variant, rows per tile).
-SHAPES = {"fp64": (1, 16), "fp32": (2, 16)}
+SHAPES = {"fp64": (1, 16), "fp32": (1, 16)}
 
 
 @dataclass
