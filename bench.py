@@ -65,6 +65,32 @@ def _traffic_per_cell(kernel, precision):
     return None
 
 
+def _profile_metric(fname, metric):
+    """A metric's value from a committed ncu summary (profiles/<fname>)."""
+    path = os.path.join(ROOT, "profiles", fname)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == metric:
+                try:
+                    return float(parts[1].replace(",", ""))
+                except ValueError:
+                    return None
+    return None
+
+
+def _issue_bound(precision):
+    """The flux kernel's second ceiling, instruction issue (FP64 pipe busy
+    fraction and issue-slot fraction), from its committed ncu summary."""
+    fname = f"k_flux_update_thacker2048_{precision}.txt"
+    pct = lambda m: (lambda v: None if v is None else v / 100.0)(_profile_metric(fname, m))  # noqa: E731
+    return {"fp64_pipe_active_frac": pct("sm__pipe_fp64_cycles_active.avg.pct_of_peak_sustained_active"),
+            "issue_active_frac": pct("smsp__issue_active.avg.pct_of_peak_sustained_active"),
+            "source": f"profiles/{fname} (ncu, one launch in the timed steps)"}
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -483,6 +509,7 @@ def main():
                                                                                f"({peak_kind})",
                          "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
                          "wetdry_dt_avg_launch_ms": wet_ms / max(wet_n, 1),
+                         "issue_bound": _issue_bound(args.precision),
                          "launch_timing": f"CUDA event pair around each of {flux_n} flux launches, in a "
                                           f"second pass of the same {args.steps} steps right after the "
                                           f"timed region"},
