@@ -50,6 +50,28 @@ def run_form(sc, precision, duration=None, arrival_depth=0.1, autotune=False, pr
     return out
 
 
+def fp32_bed(sc):
+    """A copy of the scenario whose bed is the one the FP32 form computes
+    with: per 32x32 tile the lowest interior cell as FP64 base, plus each
+    cell's offset from it rounded to FP32.  Running the FP64 path on it
+    separates the effect of the bed representation from FP32 arithmetic."""
+    import copy
+    z = np.asarray(sc.z, dtype=np.float64)
+    R, C = z.shape
+    tr, tc = (R + 31) // 32, (C + 31) // 32
+    base = np.zeros((tr, tc))
+    for i in range(tr):
+        for j in range(tc):
+            r0, r1 = max(32 * i, 1), min(32 * i + 32, R - 1)
+            c0, c1 = max(32 * j, 1), min(32 * j + 32, C - 1)
+            if r1 > r0 and c1 > c0:
+                base[i, j] = z[r0:r1, c0:c1].min()
+    b = np.repeat(np.repeat(base, 32, 0), 32, 1)[:R, :C]
+    out = copy.copy(sc)
+    out.z = b + (z - b).astype(np.float32).astype(np.float64)
+    return out
+
+
 def compare(sc, duration=None, arrival_depth=0.1, fixed_dt=None):
     a = run_form(sc, "fp64", duration, arrival_depth, fixed_dt=fixed_dt)
     b = run_form(sc, "fp32", duration, arrival_depth, fixed_dt=fixed_dt)
