@@ -276,16 +276,10 @@ int reset_tiles(tri_domain* d) {
     const int64_t sx = std::min<int64_t>(std::max(c - 1, 0) / kStripCols, ns - 1);
     pin[(size_t)(ry * ns + sx)] = 1;
   };
-  if (d->nsrc > 0) {
-    std::vector<int32_t> cells(d->nsrc);
-    TRI_CUDA_TRY(cudaMemcpy(cells.data(), d->src_cells, d->nsrc * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    for (int32_t id : cells) pin_cell(id);
-  }
-  if (d->nbc > 0) {
-    std::vector<int32_t> cells(d->nbc);
-    TRI_CUDA_TRY(cudaMemcpy(cells.data(), d->bc_cells, d->nbc * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    for (int32_t id : cells) pin_cell(id);
-  }
+  if (d->nsrc > 0)
+    for (int32_t id : d->src_cells_host) pin_cell(id);
+  if (d->nbc > 0)
+    for (int32_t id : d->bc_cells_host) pin_cell(id);
   if (d->desc.open_boundaries)
     for (int64_t ry = 0; ry < nty; ry++)
       for (int64_t sx = 0; sx < ns; sx++)
@@ -689,6 +683,7 @@ int tri_domain_set_sources(tri_domain* d, int32_t nsrc, const int32_t* cells, in
   d->src_order_host = order;
   int rc;
   if ((rc = upload_raw(d, cells, nsrc * 4, (void**)&d->src_cells)) != TRI_OK) return rc;
+  d->src_cells_host.assign(cells, cells + nsrc);
   if ((rc = upload_raw(d, order.data(), order.size() * 4, (void**)&d->src_order)) != TRI_OK) return rc;
   if ((rc = upload_raw(d, times, nrows * 8, (void**)&d->hyg_t)) != TRI_OK) return rc;
   rc = d->prec == TRI_FP64 ? upload_table<double>(d, flows, (int64_t)nsrc * nrows, &d->hyg_v)
@@ -731,6 +726,7 @@ int tri_domain_set_extbc(tri_domain* d, int32_t ncells, const int32_t* cells, co
   d->bc_order_host = order;
   int rc;
   if ((rc = upload_raw(d, cells, ncells * 4, (void**)&d->bc_cells)) != TRI_OK) return rc;
+  d->bc_cells_host.assign(cells, cells + ncells);
   if ((rc = upload_raw(d, types, ncells * 4, (void**)&d->bc_types)) != TRI_OK) return rc;
   if ((rc = upload_raw(d, start, ncells * 4, (void**)&d->bc_start)) != TRI_OK) return rc;
   if ((rc = upload_raw(d, nrows, ncells * 4, (void**)&d->bc_nrows)) != TRI_OK) return rc;

@@ -40,13 +40,13 @@ struct tri_domain {
   int32_t nsrc = 0, hyg_rows = 0;
   int32_t* src_cells = nullptr;
   int32_t* src_order = nullptr;
-  std::vector<int32_t> src_waves, src_order_host;
+  std::vector<int32_t> src_waves, src_order_host, src_cells_host;
   double* hyg_t = nullptr;
   void* hyg_v = nullptr;
   // external boundary cells
   int32_t nbc = 0;
   int32_t *bc_cells = nullptr, *bc_types = nullptr, *bc_start = nullptr, *bc_nrows = nullptr, *bc_order = nullptr;
-  std::vector<int32_t> bc_waves, bc_order_host;
+  std::vector<int32_t> bc_waves, bc_order_host, bc_cells_host;
   void *bc_v1 = nullptr, *bc_v2 = nullptr;
   // observations
   int32_t nobs = 0;

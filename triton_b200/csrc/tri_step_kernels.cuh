@@ -277,7 +277,7 @@ __device__ __forceinline__ bool nonzero_bits(float v) { return __float_as_uint(v
 // the source buffer computes exactly +0 everywhere (every face is dry-dry and
 // contributes nothing; no runoff on such a domain), and if its cells in the
 // destination buffer hold +0 already (it was all-zero two steps ago), it has
-// nothing to write.  Only lane 0's answer counts.
+// nothing to write.  Called by lane 0, which takes the tiles.
 template <typename T>
 __device__ __forceinline__ bool tile_skippable(const FluxCtx<T>& X, unsigned tile) {
   if (X.tz_src == nullptr) return false;
