@@ -102,3 +102,36 @@ def test_dry_tiles_skipped_exactly(kind, precision):
     finally:
         solo.close()
         ref.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dry_tiles_are_skipped_and_counted(precision):
+    """The mostly dry case computes well under all of its cells (the skip is
+    on), and a domain with runoff computes every cell (the skip is off)."""
+    sc = _case("walls")
+    interior = (sc.rows - 2) * (sc.cols - 2)
+    d = sc.to_domain(precision)
+    try:
+        _quiet(d)
+        d.advance(10)  # flags known after two steps
+        d.set_timing(True)
+        k, _ = d.advance(20)
+        flux_cells, wet_cells = d.get_work()
+        d.set_timing(False)
+        assert k == 20
+        assert 0 < flux_cells < 0.6 * 20 * interior, flux_cells / (20 * interior)
+        assert 0 < wet_cells < 0.8 * 20 * interior, wet_cells / (20 * interior)
+    finally:
+        d.close()
+    scenarios.runoff_table(sc, np.zeros((sc.rows - 2, sc.cols - 2), np.int32), [0.0, 1.0], [[0.0], [0.0]])
+    d = sc.to_domain(precision)
+    try:
+        _quiet(d)
+        d.advance(10)
+        d.set_timing(True)
+        k, _ = d.advance(20)
+        flux_cells, wet_cells = d.get_work()
+        d.set_timing(False)
+        assert flux_cells == wet_cells == 20 * interior
+    finally:
+        d.close()
