@@ -1,9 +1,9 @@
 """CPU tests of the drop-in host and the C ABI library (no GPU needed).
 
 * The C++ host (triton_b200/lib/triton_b200) reads a reference-format case
-  (cfg, ASCII or binary rasters, hydrograph, runoff, extbc and observation
-  files) and preprocesses it as triton_init.h does; its arrays must equal the
-  scenario the case was written from, value for value.
+  (cfg, ASCII or binary rasters, whole or partitioned, hydrograph, runoff,
+  extbc and observation files) and preprocesses it as triton_init.h does; its
+  arrays must equal the scenario the case was written from, value for value.
 * libtriton_b200.so loads and exports every symbol include/triton_b200.h
   declares.
 * The ASCII raster formatter gives printf's "%.6f" text for every double:
@@ -34,10 +34,14 @@ def _dump(tmp_path, cfg):
 
 @pytest.mark.parametrize("fmt", ["ASC", "BIN"])
 @pytest.mark.parametrize("open_b", [0, 1])
-def test_host_preprocessing_matches_scenario(tmp_path, fmt, open_b):
+@pytest.mark.parametrize("partitions", [0, 1, 3])
+def test_host_preprocessing_matches_scenario(tmp_path, fmt, open_b, partitions):
+    """partitions 0: one file per raster (input_option=SEQ); 1 or 3: a header
+    file and one file per partition (input_option=PAR), 3 being rows split as
+    for three ranks and stacked again by the host."""
     from triton_b200 import scenarios
     sc = scenarios.mixed(rows=23, cols=37, seed=9 + open_b, open_boundaries=open_b, duration=5.0)
-    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt=fmt)
+    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt=fmt, partitions=partitions)
     info, rd = _dump(tmp_path, cfg)
     R, C = int(info["rows"]), int(info["cols"])
     assert (R, C) == (sc.rows, sc.cols)

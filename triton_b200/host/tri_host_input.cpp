@@ -340,6 +340,28 @@ static int src_row(double y, double yll, double cell, int nrows) {
 
 static std::string two(int v) { return v < 10 ? "0" + std::to_string(v) : std::to_string(v); }
 
+// Partitioned input (input_option=PAR, triton_init.h:359-717): raster <base>
+// is stored as <base>_NN<ext>, one file per partition (NN: the rank, two
+// digits), without the DEM header (that comes from header_filename).  A
+// single rank reads _00 holding the whole domain.  Files written for N ranks
+// hold row slabs as create_local_dims makes them (mpi_utils.h:73-89: R/N
+// rows each, one more for each of the first R%N ranks); they are read in rank
+// order and stacked, so a case partitioned for N ranks runs on one GPU.
+template <typename T, typename Reader>
+static std::vector<T> read_parts(const std::string& base, const std::string& ext, int R, int C, Reader read) {
+  int n = 0;
+  while (n < 100 && std::ifstream(base + "_" + two(n) + ext).good()) n++;
+  if (n == 0) throw InputError("Error reading file: " + base + "_00" + ext);
+  std::vector<T> out;
+  out.reserve((size_t)R * C);
+  for (int p = 0; p < n; p++) {
+    const int rows = R / n + (p < R % n ? 1 : 0);
+    const std::vector<T> part = read(base + "_" + two(p) + ext, rows, C);
+    out.insert(out.end(), part.begin(), part.end());
+  }
+  return out;
+}
+
 Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int checkpoint_id) {
   Problem P;
   P.project_dir = root_dir(argv0.c_str());
@@ -360,8 +382,11 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
   Args& a = P.args;
   a = get_args(P.cfg_content);
   P.simtime = a.sim_start_time;
-  if (a.input_option != "SEQ") throw InputError("input_option=" + a.input_option + " is not supported (SEQ only)");
+  const bool par = a.input_option == "PAR";
+  if (!par && a.input_option != "SEQ")
+    throw InputError("input_option=" + a.input_option + " is not supported (SEQ or PAR)");
   const bool asc = a.input_format == "ASC";
+  auto raster_part = [asc](const std::string& path, int r, int c) { return read_raster(path, r, c, asc); };
 
   // read_inflows (triton_init.h:140-167)
   std::vector<std::vector<double>> hyg, roff;
@@ -380,13 +405,22 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
   }
 
   // DEM and fields (triton_init.h:171-353)
-  P.dem = read_dem_header(a.dem_filename, asc);
+  // the header of a partitioned DEM is its own ASCII file (triton_init.h:171-191)
+  P.dem = par ? read_dem_header(a.header_filename, true) : read_dem_header(a.dem_filename, asc);
   const int R = P.dem.nrows, C = P.dem.ncols;
-  if (R <= 0 || C <= 0) throw InputError("Invalid DEM dimensions in " + a.dem_filename);
+  if (R <= 0 || C <= 0) throw InputError("Invalid DEM dimensions in " + (par ? a.header_filename : a.dem_filename));
   const int Rp = R + 2, Cp = C + 2;
   P.rows = Rp;
   P.cols = Cp;
-  P.z = pad(read_dem(a.dem_filename, R, C, asc), R, C, 0.0);
+  if (par)  // DEM partitions: ASCII without a header and unchecked, binary with its two-value header
+    P.z = pad(read_parts<double>(a.dem_filename, ".dem", R, C,
+                                 [asc](const std::string& path, int r, int c) {
+                                   return asc ? read_ascii<double>(path, r, c, 0, false)
+                                              : read_binary<double>(path, r, c, 2, true);
+                                 }),
+              R, C, 0.0);
+  else
+    P.z = pad(read_dem(a.dem_filename, R, C, asc), R, C, 0.0);
   if (!a.open_boundaries) {  // closed walls: DEM ghosts 1e6 (matrix.h:929-945)
     for (int i = 0; i < Rp; i++) P.z[(size_t)i * Cp] = P.z[(size_t)i * Cp + Cp - 1] = 1e6;
     for (int j = 0; j < Cp; j++) P.z[j] = P.z[(size_t)(Rp - 1) * Cp + j] = 1e6;
@@ -395,7 +429,7 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
   }
   std::vector<double> nin;
   if (!a.n_infile.empty()) {
-    nin = read_raster(a.n_infile, R, C, asc);
+    nin = par ? read_parts<double>(a.n_infile, ".mann", R, C, raster_part) : read_raster(a.n_infile, R, C, asc);
   } else {
     nin.assign((size_t)R * C, 0.0);
     for (double& v : nin) v = v + a.const_mann;
@@ -405,7 +439,8 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
   for (double& v : P.n2) v = v * v;
   auto field = [&](const std::string& f) {
     if (f.empty()) return std::vector<double>((size_t)Rp * Cp, 0.0);
-    std::vector<double> v = pad(read_raster(f, R, C, asc), R, C, 0.0);
+    std::vector<double> v =
+        pad(par ? read_parts<double>(f, ".out", R, C, raster_part) : read_raster(f, R, C, asc), R, C, 0.0);
     if (a.open_boundaries) copy_ghosts(v, Rp, Cp);
     return v;
   };
@@ -414,7 +449,12 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
   P.qy = field(a.qy_infile);
   std::vector<int32_t> rin;
   if (!a.runoff_map.empty()) {
-    std::vector<int32_t> r = read_raster_int(a.runoff_map, R, C, asc);
+    std::vector<int32_t> r =
+        par ? read_parts<int32_t>(a.runoff_map, ".rmap", R, C,
+                                  [asc](const std::string& path, int rr, int cc) {
+                                    return read_raster_int(path, rr, cc, asc);
+                                  })
+            : read_raster_int(a.runoff_map, R, C, asc);
     rin.assign((size_t)Rp * Cp, 0);
     for (int i = 0; i < R; i++)
       for (int j = 0; j < C; j++) rin[(size_t)(i + 1) * Cp + j + 1] = r[(size_t)i * C + j];

@@ -495,38 +495,65 @@ def _fmt(v):
     return s
 
 
+def _write_parts(base, suffix, a, fmt, parts, dtype=np.float64):
+    """Partitioned raster (input_option=PAR): `parts` files <base>_NN<suffix>
+    holding row slabs split as the reference splits rows among ranks
+    (create_local_dims, mpi_utils.h:73-89), each without a DEM header; a
+    binary file starts with its slab's rows and cols."""
+    R = a.shape[0]
+    r0 = 0
+    for p in range(parts):
+        rows = R // parts + (1 if p < R % parts else 0)
+        _write_raster(f"{base}_{p:02d}{suffix}", a[r0:r0 + rows], fmt, dtype=dtype)
+        r0 += rows
+
+
 def write_case(sc, directory, fmt="BIN", output_format="BIN", output_folder="output", name=None,
-               max_value_print=""):
+               max_value_print="", partitions=0):
     """Writes `sc` as a reference-format case (cfg + inputs) into `directory`
     and returns the cfg path.  Paths inside the cfg are absolute.  The
     reference recovers the same padded arrays and tables from these files
     (initial fields, walls, Manning squared, forcing unit conversions, cell
-    coordinates -> indices via calc_src_col/row)."""
+    coordinates -> indices via calc_src_col/row).  partitions > 0 writes the
+    rasters partitioned (input_option=PAR): an ASCII header file and one file
+    per partition and field (triton_init.h:359-717)."""
     os.makedirs(directory, exist_ok=True)
     name = name or sc.name
     R, C = sc.rows - 2, sc.cols - 2
     dx = sc.dx
     P = lambda f: os.path.abspath(os.path.join(directory, f))
     ext = "bin" if fmt == "BIN" else "asc"
-    _write_raster(P(f"{name}.dem.{ext}"), sc.z[1:-1, 1:-1], fmt,
-                  dem_header=[float(C), float(R), sc.xll, sc.yll, dx, -9999.0] if fmt == "BIN" else
-                  [C, R, sc.xll, sc.yll, dx, -9999])
-    _write_raster(P(f"{name}.h.{ext}"), sc.h[1:-1, 1:-1], fmt)
-    _write_raster(P(f"{name}.qx.{ext}"), sc.qx[1:-1, 1:-1], fmt)
-    _write_raster(P(f"{name}.qy.{ext}"), sc.qy[1:-1, 1:-1], fmt)
     mann = sc.meta.get("mann")
     if mann is None:
         mann = np.sqrt(sc.n2[1:-1, 1:-1])
-    _write_raster(P(f"{name}.mann.{ext}"), mann, fmt)
+    if partitions > 0:
+        with open(P(f"{name}.header"), "w") as f:
+            f.write(f"ncols {C}\nnrows {R}\nxllcorner {sc.xll!r}\nyllcorner {sc.yll!r}\ncellsize {dx!r}\n"
+                    f"NODATA_value -9999\n")
+        names = {k: P(f"{name}_{k}") for k in ("dem", "h", "qx", "qy", "mann")}
+        _write_parts(names["dem"], ".dem", sc.z[1:-1, 1:-1], fmt, partitions)
+        _write_parts(names["h"], ".out", sc.h[1:-1, 1:-1], fmt, partitions)
+        _write_parts(names["qx"], ".out", sc.qx[1:-1, 1:-1], fmt, partitions)
+        _write_parts(names["qy"], ".out", sc.qy[1:-1, 1:-1], fmt, partitions)
+        _write_parts(names["mann"], ".mann", mann, fmt, partitions)
+    else:
+        names = {k: P(f"{name}.{k}.{ext}") for k in ("dem", "h", "qx", "qy", "mann")}
+        _write_raster(names["dem"], sc.z[1:-1, 1:-1], fmt,
+                      dem_header=[float(C), float(R), sc.xll, sc.yll, dx, -9999.0] if fmt == "BIN" else
+                      [C, R, sc.xll, sc.yll, dx, -9999])
+        _write_raster(names["h"], sc.h[1:-1, 1:-1], fmt)
+        _write_raster(names["qx"], sc.qx[1:-1, 1:-1], fmt)
+        _write_raster(names["qy"], sc.qy[1:-1, 1:-1], fmt)
+        _write_raster(names["mann"], mann, fmt)
 
     def xy(r, c):
         return sc.xll + (c + 0.5) * dx, sc.yll + (R - r - 0.5) * dx
 
     cfg = {
-        "dem_filename": P(f"{name}.dem.{ext}"), "input_format": fmt, "input_option": "SEQ",
+        "dem_filename": names["dem"], "input_format": fmt, "input_option": "PAR" if partitions > 0 else "SEQ",
         "outfile_pattern": "%s/%s/%s_%02d_%02d", "output_format": output_format, "output_option": "SEQ",
-        "output_folder": output_folder, "n_infile": P(f"{name}.mann.{ext}"), "const_mann": "0.0",
-        "h_infile": P(f"{name}.h.{ext}"), "qx_infile": P(f"{name}.qx.{ext}"), "qy_infile": P(f"{name}.qy.{ext}"),
+        "output_folder": output_folder, "n_infile": names["mann"], "const_mann": "0.0",
+        "h_infile": names["h"], "qx_infile": names["qx"], "qy_infile": names["qy"],
         "num_sources": "0", "num_runoffs": "0", "num_extbc": "0", "time_series_flag": str(int(sc.time_series)),
         "print_option": "huv", "sim_start_time": "0", "sim_duration": repr(float(sc.sim_duration)),
         "checkpoint_id": "0", "time_increment_fixed": "0", "time_step": repr(float(sc.time_step)),
@@ -562,15 +589,21 @@ def write_case(sc, directory, fmt="BIN", output_format="BIN", output_folder="out
             for t, row in zip(s["times_h"], s["flows_rows"]):
                 f.write(",".join([repr(float(t))] + [repr(float(v)) for v in row]) + "\n")
         cfg.update(num_sources=str(len(rcs)), src_loc_file=P(f"{name}.src"), hydrograph_filename=P(f"{name}.hyg"))
+    if partitions > 0:
+        cfg["header_filename"] = P(f"{name}.header")
     if sc.runoff is not None:
         r = sc.runoff
-        _write_raster(P(f"{name}.rmap.{ext}"), r["zone"][1:-1, 1:-1], fmt, dtype=np.int32)
+        if partitions > 0:
+            rmap = P(f"{name}_rmap")
+            _write_parts(rmap, ".rmap", r["zone"][1:-1, 1:-1], fmt, partitions, dtype=np.int32)
+        else:
+            rmap = P(f"{name}.rmap.{ext}")
+            _write_raster(rmap, r["zone"][1:-1, 1:-1], fmt, dtype=np.int32)
         with open(P(f"{name}.roff"), "w") as f:
             f.write("% Time(hr), Rate(mm/hr)\n")
             for t, row in zip(r["times_h"], r["rates_mm_h"]):
                 f.write(",".join([repr(float(t))] + [repr(float(v)) for v in np.atleast_1d(row)]) + "\n")
-        cfg.update(num_runoffs=str(int(r["nzones"])), runoff_filename=P(f"{name}.roff"),
-                   runoff_map=P(f"{name}.rmap.{ext}"))
+        cfg.update(num_runoffs=str(int(r["nzones"])), runoff_filename=P(f"{name}.roff"), runoff_map=rmap)
     segs = getattr(sc, "_segments", None)
     if segs:
         lines = ["% BC Type, X1, Y1, X2, Y2, BC"]
