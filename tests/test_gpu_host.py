@@ -69,13 +69,18 @@ def _read_bin(path):
     return v[2:].reshape(r, c)
 
 
-def test_synthetic_case_matches_reference_executable(tmp_path):
+@pytest.mark.parametrize("fmt,partitions", [("BIN", 0), ("ASC", 1)])
+def test_synthetic_case_matches_reference_executable(tmp_path, fmt, partitions):
+    """partitions 1: the rasters as partitioned input (input_option=PAR, a
+    header file and one file per field), which the reference reads on one
+    rank as it would on many."""
     if not os.path.exists(REF):
         pytest.skip("reference executable not built")
     from triton_b200 import scenarios
     sc = scenarios.mixed(rows=45, cols=71, seed=17, open_boundaries=0, friction=True, duration=12.0)
     outs = {}
-    cfg = scenarios.write_case(sc, str(tmp_path / "input"), fmt="BIN", output_format="ASC", max_value_print="h")
+    cfg = scenarios.write_case(sc, str(tmp_path / "input"), fmt=fmt, output_format="ASC", max_value_print="h",
+                               partitions=partitions)
     for name, exe in (("ours", EXE), ("ref", REF)):
         base = tmp_path / name
         (base / "bin").mkdir(parents=True)
