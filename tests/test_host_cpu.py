@@ -87,6 +87,15 @@ def test_host_rejects_bad_inputs(tmp_path):
     p = subprocess.run([EXE, "--dump-problem", str(tmp_path), str(tmp_path / "nope.cfg")], capture_output=True,
                        text=True, timeout=60)
     assert p.returncode != 0 and "Error reading file" in p.stderr
+    # partitioned input without its first partition, and an unknown input option
+    cfg3 = scenarios.write_case(sc2, str(tmp_path / "case3"), fmt="BIN", partitions=2)
+    os.remove(tmp_path / "case3" / "mixed_dem_00.dem")
+    p = subprocess.run([EXE, "--dump-problem", str(tmp_path), cfg3], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "mixed_dem_00.dem" in p.stderr
+    cfg4 = tmp_path / "case3" / "other.cfg"
+    cfg4.write_text(open(cfg3).read().replace("input_option=PAR", "input_option=XYZ"))
+    p = subprocess.run([EXE, "--dump-problem", str(tmp_path), str(cfg4)], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "input_option=XYZ is not supported" in p.stderr
 
 
 def test_cfg_parser_rules(tmp_path):
