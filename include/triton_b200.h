@@ -188,6 +188,13 @@ int tri_domain_get_timing(tri_domain* d, double* flux_ms, int32_t* flux_launches
  * hold only zeros, whose update is exactly the identity).  No reference
  * counterpart (the reference updates every cell every step). */
 int tri_domain_get_work(tri_domain* d, int64_t* flux_cells, int64_t* wetdry_cells);
+/* Test hook for the bounded device waits (no reference counterpart; the
+ * reference's kernels never wait).  While polls > 0, every step's wet-dry
+ * launch also waits, at most 'polls' polls, on a barrier that nothing
+ * completes; the wait gives up, the launch records a device status, and
+ * tri_domain_advance returns TRI_E_TIMEOUT once the steps have run (the
+ * computation itself is untouched).  0 (the default) turns it off. */
+int tri_domain_set_wait_test(tri_domain* d, uint32_t polls);
 
 /* Launch-shape autotuner of the flux kernel.  Runs trial_steps steps of the
  * domain's own state for every candidate (register budget x tile height),
@@ -286,7 +293,9 @@ int tri_kernel_copy_info_to_exterior_boundaries_north_south_f64(int size, int nr
 /* compute_extbc_values: cells that touch the same cell (corners shared by two
  * segments, repeated cells) are applied in index order, as the reference's
  * serial build does; to schedule them the entry reads the cell list back to
- * the host, so it synchronizes 'stream'. */
+ * the host, so it synchronizes 'stream'.  The order is cached per host thread
+ * and device, in device memory allocated on first use and grown for longer
+ * lists (freed when the thread exits). */
 int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double dt, double* h, double* qx, double* qy,
                                         const double* dem, const double* n, const int32_t* relative_index,
                                         const int32_t* extbctype, const int32_t* start_index,
@@ -305,7 +314,9 @@ int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double d
  * (which may load the library's device code); make it before any stream
  * capture.  The array is shared by every call on a device: calls that
  * overlap in time (from other host threads, or while kernels of an earlier
- * call with another cell list still run on another stream) race on it. */
+ * call with another cell list still run on another stream) race on it.  A
+ * call that writes a new order waits for the copy to land before it returns,
+ * so a later call with the same list, on any stream, finds it in place. */
 #define TRI_NOALLOC_EXTBC_MAX_CELLS 65536
 int tri_kernel_compute_extbc_values_noalloc_f64(int size, int nrows, int ncols, double dt, double* h, double* qx,
                                                 double* qy, const double* dem, const double* n,

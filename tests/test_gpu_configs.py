@@ -1,0 +1,112 @@
+"""Parity at the full sizes of the plain FP64 workloads, on the GPU.
+
+* Circular dam break, 512 x 512, dx 1 m, 10 m of water within 50 m of the
+  centre, dry outside, flat frictionless bed, closed walls, CFL 0.5, 5 s:
+  the drop-in executable and the reference executable (built from its own
+  sources, oracle/_ref) run the same case files; the binary outputs must be
+  identical (no cube root is taken: bit-exact).
+* Thacker planar oscillation in a paraboloid bowl, 2048 x 2048, dx 4 m,
+  h0 10 m, a 3000 m, rim surface amplitude 0.5 m, closed walls, CFL 0.5: the
+  first 40 s (about 205 steps, two prints) against the reference executable,
+  bit-exact; and the whole two periods (about 13 800 steps) on the GPU
+  against Thacker's analytic solution away from the moving shoreline.
+
+The reference runs its OpenMP build without FMA contraction
+(oracle/_ref/triton_ref_mt), which computes the same bits as its serial
+build on these cases (no two sources or boundary cells share a cell)."""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+import pytest
+
+from tests import _cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_both(tmp_path, sc):
+    if not os.path.exists(_cases.REF_MT):
+        pytest.skip("reference executable not built")
+    from triton_b200 import scenarios
+    cfg = scenarios.write_case(sc, str(tmp_path / "input"), fmt="BIN", output_format="BIN", max_value_print="h")
+    outs = {}
+    for name, exe in (("ours", _cases.EXE), ("ref", _cases.REF_MT)):
+        base = str(tmp_path / name)
+        _cases.run_exe(_cases.project(base, exe), base, [cfg], timeout=1800, threads=os.cpu_count())
+        outs[name] = os.path.join(base, "output", "bin")
+    return outs
+
+
+def _assert_identical(outs, n_files):
+    names = sorted(os.listdir(outs["ref"]))
+    assert len(names) == n_files and sorted(os.listdir(outs["ours"])) == names
+    for f in names:
+        a, b = _cases.read_bin(os.path.join(outs["ours"], f)), _cases.read_bin(os.path.join(outs["ref"], f))
+        bad = a != b
+        if bad.any():
+            i = tuple(np.argwhere(bad)[0])
+            raise AssertionError(f"{f}: {bad.sum()} cells differ, first at {i}: ours {a[i]!r} reference {b[i]!r}")
+
+
+def test_dambreak_512_matches_reference_executable(tmp_path):
+    from triton_b200 import scenarios
+    sc = scenarios.dambreak(n=512, dx=1.0, radius=50.0, depth=10.0, duration=5.0)
+    outs = _run_both(tmp_path, sc)
+    _assert_identical(outs, 4)  # H, QX, QY, MH at t = 5 s
+    h = _cases.read_bin(os.path.join(outs["ours"], "H_01_00.out"))
+    assert (h > sc.hextra).sum() > 2 * math.pi * 50.0 ** 2  # the front has moved out
+
+
+def test_thacker_2048_first_40s_matches_reference_executable(tmp_path):
+    from triton_b200 import scenarios
+    sc = scenarios.thacker(n=2048, dx=4.0, h0=10.0, a=3000.0, amplitude=0.5)
+    sc.sim_duration, sc.print_interval = 40.0, 20.0
+    outs = _run_both(tmp_path, sc)
+    _assert_identical(outs, 8)  # H, QX, QY, MH at t = 20 s and 40 s
+
+
+# Away from the shoreline: cells where the analytic depth is at least 0.5 m
+# (about 19 cells inland of the moving shoreline).  Bounds on the depth
+# error of this first-order scheme at dx = 4 m over the whole run:
+ANALYTIC_MAX = 0.05  # m
+ANALYTIC_RMS = 0.01  # m
+
+
+def test_thacker_2048_two_periods_against_analytic_solution():
+    """Thacker (1981), planar surface: w = h0 + (eta h0/a^2)(2x'cos wt +
+    2y'sin wt - eta), u = -eta w sin wt, v = eta w cos wt, w = sqrt(2 g h0)/a;
+    the rim surface amplitude A = 2 eta h0 / a = 0.5 m gives eta = 75 m, the
+    period is 2 pi / w = 1345.7 s.  Compared at every quarter period."""
+    from tests._harness import domain_bookkeeping, EV_END, EV_PRINT
+    from triton_b200 import scenarios
+    sc = scenarios.thacker(n=2048, dx=4.0, h0=10.0, a=3000.0, amplitude=0.5, periods=2.0)
+    m = sc.meta
+    sc.print_interval = m["period"] / 4
+    X, Y = scenarios._centres(m["n"], m["n"], sc.dx)
+    d = sc.to_domain()
+    results = []
+    try:
+        while True:
+            n, ev = d.advance(1 << 30)
+            c = d.get_clock()
+            if ev & EV_PRINT:
+                _, he, _, _, _ = scenarios.thacker_state(X, Y, c.simtime, m["h0"], m["a"], m["eta"], m["xc"], m["yc"])
+                h = d.download("h")[1:-1, 1:-1]
+                far = he >= 0.5
+                err = np.abs(h - he)[far]
+                results.append((c.simtime, float(err.max()), float(np.sqrt((err ** 2).mean())), int(far.sum())))
+            domain_bookkeeping(d, ev)
+            if ev & EV_END or n == 0:
+                break
+    finally:
+        d.close()
+    for t, mx, rms, cells in results:
+        print(f"t = {t:8.2f} s ({t / m['period']:.2f} periods): max |h - exact| {mx:.4e} m, RMS {rms:.4e} m "
+              f"over {cells} cells")
+    assert len(results) == 8 and abs(results[-1][0] - 2 * m["period"]) < 1e-6
+    for t, mx, rms, _ in results:
+        assert mx <= ANALYTIC_MAX and rms <= ANALYTIC_RMS, (t, mx, rms)
+    assert math.isfinite(results[-1][1])

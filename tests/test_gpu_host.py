@@ -108,3 +108,70 @@ def test_synthetic_case_matches_reference_executable(tmp_path, fmt, partitions):
                 assert abs(float(la.split("=")[1]) - float(lb.split("=")[1])) <= 1e-9 * max(1.0, abs(float(lb.split("=")[1])))
             else:
                 assert la == lb, (f, la, lb)
+
+
+def test_checkpoint_resume_matches_reference_executable(tmp_path):
+    """Resume from a checkpoint (triton_init.h:24-27,98-101,303-353): each
+    executable runs a case with three prints, then resumes it from print 1
+    (command line <cfg> <threads> 1) after the restart cfg it wrote there
+    (output.h:754-811) is placed where the reference looks for it
+    (<project>//cfg/config_1.cfg: the folder name is still empty when that
+    path is formed).  The resumed runs must agree with each other (binary
+    outputs within 1e-9 of each field's scale, identical wet/dry masks,
+    the same series text and restart cfgs) and each with its own
+    uninterrupted run (the checkpoint holds the state exactly)."""
+    if not os.path.exists(REF):
+        pytest.skip("reference executable not built")
+    from triton_b200 import scenarios
+    sc = scenarios.mixed(rows=45, cols=71, seed=23, open_boundaries=0, friction=True, duration=12.0)
+    cfg = scenarios.write_case(sc, str(tmp_path / "input"), fmt="BIN", output_format="BIN", max_value_print="h")
+    runs = {}
+    for name, exe in (("ours", EXE), ("ref", REF)):
+        base = tmp_path / name
+        (base / "bin").mkdir(parents=True)
+        os.symlink(exe, base / "bin" / "triton.exe")
+        _run(str(base / "bin" / "triton.exe"), base, cfg)
+        full = {f: _read_bin(base / "output" / "bin" / f) for f in os.listdir(base / "output" / "bin")}
+        (base / "cfg").mkdir()
+        shutil.copy(base / "output" / "cfg" / "config_1.cfg", base / "cfg" / "config_1.cfg")
+        env = dict(os.environ, LD_LIBRARY_PATH=os.path.join(ROOT, "triton_b200", "lib"))
+        p = subprocess.run([str(base / "bin" / "triton.exe"), cfg, "1", "1"], cwd=base, capture_output=True,
+                           text=True, timeout=900, env=env)
+        assert p.returncode == 0, p.stderr[-3000:]
+        resumed = {f: _read_bin(base / "output" / "bin" / f) for f in os.listdir(base / "output" / "bin")}
+        assert sorted(full) == sorted(resumed) and len(full) == 12  # H/QX/QY/MH at prints 1-3
+        for f in full:
+            assert np.array_equal(full[f], resumed[f]), f"{name}: resumed {f} differs from the uninterrupted run"
+        runs[name] = (base, resumed)
+    (ba, ra), (bb, rb) = runs["ours"], runs["ref"]
+    for f in sorted(rb):
+        a, b = ra[f], rb[f]
+        scale = max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-9 * scale, f"{f}: {np.abs(a - b).max() / scale:.2e}"
+        if f.startswith("H_"):
+            assert np.array_equal(a > sc.hextra, b > sc.hextra), f"{f}: wet mask differs"
+    for f in ("H_at_Xsec.txt", "QX_at_Xsec.txt", "QY_at_Xsec.txt"):
+        ta = (ba / "output" / "series" / f).read_text().splitlines()
+        tb = (bb / "output" / "series" / f).read_text().splitlines()
+        assert len(ta) == len(tb) and ta[0] == tb[0], f
+        for la, lb in zip(ta[1:], tb[1:]):
+            va, vb = np.array(la.split(","), float), np.array(lb.split(","), float)
+            assert va.shape == vb.shape and np.allclose(va, vb, rtol=0, atol=2e-6), (f, la, lb)
+    _compare_restart_cfgs(ba / "output" / "cfg", bb / "output" / "cfg")
+
+
+def _compare_restart_cfgs(da, db):
+    """Restart cfgs equal line for line; the simtime and mean dt they carry
+    within 1e-9 (the state, hence dt, may differ in the last bits where cube
+    roots are taken)."""
+    names = sorted(os.listdir(db))
+    assert names and sorted(os.listdir(da)) == names
+    for f in names:
+        ca, cb = (da / f).read_text().splitlines(), (db / f).read_text().splitlines()
+        assert len(ca) == len(cb), f
+        for la, lb in zip(ca, cb):
+            if la.startswith(("sim_start_time=", "time_step=")):
+                va, vb = float(la.split("=")[1]), float(lb.split("=")[1])
+                assert abs(va - vb) <= 1e-9 * max(1.0, abs(vb)), (f, la, lb)
+            else:
+                assert la == lb, (f, la, lb)

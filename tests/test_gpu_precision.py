@@ -77,3 +77,16 @@ def test_fp32_domain_roundtrip_of_bed():
         d.close()
     inner = sc.z[1:-1, 1:-1]
     assert np.abs(z[1:-1, 1:-1] - inner).max() < 2e-5
+
+
+@pytest.mark.xfail(strict=False, reason="the FP32 form's targets (1e-3 m max depth error, 1e-6 relative volume "
+                                        "error) are not met with point sources: see the bounds measured above")
+def test_fp32_source_watershed_at_target_bounds():
+    """The stated targets of the FP32 form, on the source watershed above.
+    Kept visible as an expected failure while the measured errors (max depth
+    1.7e-3 m, volume 1.9e-6 .. 2.5e-6) exceed them."""
+    from triton_b200 import precision, scenarios
+    sc = scenarios.watershed(n=192, dx=10.0, seed=3, duration=1800.0, nsrc=2, peak_flow=20.0)
+    r = precision.compare(sc)
+    assert r["max_depth_error_m"] <= 1e-3, r
+    assert r["volume_rel_error"] <= 1e-6, r

@@ -67,6 +67,46 @@ def test_host_preprocessing_matches_scenario(tmp_path, fmt, open_b, partitions):
     assert float(info["init_dt"]) == sc.init_dt()
 
 
+@pytest.mark.parametrize("partitions,output_option", [(0, "SEQ"), (0, "PAR"), (1, "SEQ"), (3, "SEQ"), (3, "PAR")])
+def test_host_reads_checkpoint_rasters(tmp_path, partitions, output_option):
+    """A restart cfg (checkpoint_id > 0) replaces the initial depth,
+    discharges and max depth with the checkpoint's binary rasters
+    <output_folder>/bin/<H|QX|QY|MH>_<id>_<rank>.out.  Sequential input reads
+    rank 00's file holding the whole domain, and only when output_option is
+    SEQ (triton_init.h:303-353; otherwise the initial fields stand);
+    partitioned input reads one file per rank with that rank's rows
+    (triton_init.h:577-626), here written as 1 or 3 ranks would write them
+    and stacked in rank order."""
+    from triton_b200 import scenarios
+    sc = scenarios.mixed(rows=23, cols=37, seed=11, open_boundaries=0, duration=5.0)
+    cfg = scenarios.write_case(sc, str(tmp_path / "case"), fmt="BIN", partitions=partitions)
+    text = open(cfg).read().replace("checkpoint_id=0", "checkpoint_id=1").replace(
+        "output_option=SEQ", f"output_option={output_option}") + "max_value_print_option=h\n"
+    open(cfg, "w").write(text)
+    base = tmp_path / "proj"
+    (base / "bin").mkdir(parents=True)
+    os.symlink(EXE, base / "bin" / "triton.exe")
+    (base / "output" / "bin").mkdir(parents=True)
+    rng = np.random.default_rng(1)
+    R, C = sc.rows - 2, sc.cols - 2
+    hot = {k: rng.random((R, C)) for k in ("H", "QX", "QY", "MH")}
+    for k, a in hot.items():
+        if partitions == 0:
+            scenarios._write_raster(str(base / "output" / "bin" / f"{k}_01_00.out"), a, "BIN")
+        else:  # per-rank slabs as create_local_dims splits rows (mpi_utils.h:73-89)
+            scenarios._write_parts(str(base / "output" / "bin" / f"{k}_01"), ".out", a, "BIN", partitions)
+    out = tmp_path / "dump"
+    out.mkdir()
+    p = subprocess.run([str(base / "bin" / "triton.exe"), "--dump-problem", str(out), cfg], capture_output=True,
+                       text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    rd = lambda n: np.fromfile(out / n, dtype=np.float64).reshape(sc.rows, sc.cols)[1:-1, 1:-1]
+    read = partitions > 0 or output_option == "SEQ"
+    for k, name in (("H", "h"), ("QX", "qx"), ("QY", "qy"), ("MH", "maxh")):
+        want = hot[k] if read else (sc.h if k == "MH" else getattr(sc, name))[1:-1, 1:-1]
+        assert np.array_equal(rd(f"{name}.f64"), want), (k, partitions, output_option)
+
+
 def test_host_rejects_bad_inputs(tmp_path):
     from triton_b200 import scenarios
     sc = scenarios.mixed(rows=11, cols=13, seed=2, duration=2.0)

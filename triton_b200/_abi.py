@@ -82,6 +82,7 @@ _SIGS = {
     "tri_domain_set_timing": (C.c_int, [_vp, C.c_int32]),
     "tri_domain_get_timing": (C.c_int, [_vp, _dp, _ip, _dp, _ip]),
     "tri_domain_get_work": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "tri_domain_set_wait_test": (C.c_int, [_vp, C.c_uint32]),
     "tri_domain_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_domain_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
     "tri_domain_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),

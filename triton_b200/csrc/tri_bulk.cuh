@@ -13,6 +13,7 @@ namespace tri {
 constexpr uint32_t kSpinLimit = 1u << 24;
 // Device-side status codes (DevClock::status).
 constexpr int32_t kStatusStageTimeout = 1;
+constexpr int32_t kStatusTestWait = 2;  // the wait of the test hook gave up (tri_domain_set_wait_test)
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -36,10 +37,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
       : "memory");
 }
 
-// One bounded wait for the phase with the given parity; true once complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// One bounded wait for the phase with the given parity: at most 'limit'
+// polls; true once complete, false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kSpinLimit) {
   const uint32_t a = smem_addr(bar);
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -51,6 +53,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (done) return true;
   }
   return false;
+}
+
+// Arrives on 'bar' and adds 'bytes' to the transaction count of its phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
 }
 
 // Copies 'bytes' (a multiple of 16) from global 'src' (16-byte aligned) to

@@ -1039,6 +1039,12 @@ int tri_domain_mass_balance(tri_domain* d, double* out) {
   return TRI_OK;
 }
 
+int tri_domain_set_wait_test(tri_domain* d, uint32_t polls) {
+  TRI_CHECK_ARG(d, "null domain");
+  d->mirror->wait_test = polls;  // reaches the device with the clock at the next advance
+  return TRI_OK;
+}
+
 int tri_domain_track_arrival(tri_domain* d, double depth) {
   TRI_CHECK_ARG(d, "null domain");
   TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));

@@ -351,6 +351,39 @@ int launched() {
   return TRI_OK;
 }
 
+// Application order of tri_kernel_compute_extbc_values_f64 for one host
+// thread on one device: the cell list it was built for, its waves, and its
+// device copy (allocated on that device, grown when a longer list comes).
+struct ExtbcOrderCache {
+  std::vector<int32_t> cells, order, waves;
+  int32_t* d_order = nullptr;
+  size_t cap = 0;
+};
+
+// Per host thread (each thread's calls are ordered on its own streams), per
+// device.  At thread exit the device copies are freed; a failure there (the
+// runtime may be shutting down at process exit) is ignored.
+struct ExtbcOrderCaches {
+  std::vector<std::pair<int, ExtbcOrderCache>> by_device;
+  ~ExtbcOrderCaches() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    for (auto& e : by_device) {
+      if (!e.second.d_order) continue;
+      if (cudaSetDevice(e.first) == cudaSuccess) cudaFree(e.second.d_order);
+    }
+    cudaSetDevice(cur);
+  }
+};
+
+ExtbcOrderCache& extbc_cache_of(int dev) {
+  static thread_local ExtbcOrderCaches caches;
+  for (auto& e : caches.by_device)
+    if (e.first == dev) return e.second;
+  caches.by_device.emplace_back(dev, ExtbcOrderCache());
+  return caches.by_device.back().second;
+}
+
 }  // namespace
 
 extern "C" {
@@ -456,32 +489,37 @@ int tri_kernel_compute_extbc_values_f64(int size, int nrows, int ncols, double d
   // The cell list decides the application order: cells that touch the same
   // cell run in index order (the reference's serial semantics), the rest in
   // parallel.  The list is small (boundary cells); its waves are cached per
-  // list contents.
+  // host thread and device (a device pointer is only valid on the device it
+  // was allocated on), keyed by the list's contents.
   cudaStream_t s = as_stream(stream);
-  static thread_local std::vector<int32_t> last_cells, order, waves;
-  static thread_local int32_t* d_order = nullptr;
-  static thread_local size_t d_order_cap = 0;
+  int dev = 0;
+  TRI_CUDA_TRY(cudaGetDevice(&dev));
+  ExtbcOrderCache& cache = extbc_cache_of(dev);
   std::vector<int32_t> cells((size_t)size);
   TRI_CUDA_TRY(cudaMemcpyAsync(cells.data(), relative_index, size * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   TRI_CUDA_TRY(cudaStreamSynchronize(s));
-  if (cells != last_cells) {
+  if (cells != cache.cells) {
     std::vector<std::vector<int64_t>> touch((size_t)size);
     for (int i = 0; i < size; i++) {
       const int64_t ii = cells[i];
       touch[i] = extbc_touches(ii, nrows, ncols);
     }
-    build_waves(touch, order, waves);
-    if (d_order_cap < order.size()) {
-      if (d_order) cudaFree(d_order);
-      TRI_CUDA_TRY(cudaMalloc((void**)&d_order, order.size() * sizeof(int32_t)));
-      d_order_cap = order.size();
+    cache.cells.clear();  // stays invalid if an allocation or copy below fails
+    build_waves(touch, cache.order, cache.waves);
+    if (cache.cap < cache.order.size()) {
+      if (cache.d_order) cudaFree(cache.d_order);
+      cache.d_order = nullptr;
+      cache.cap = 0;
+      TRI_CUDA_TRY(cudaMalloc((void**)&cache.d_order, cache.order.size() * sizeof(int32_t)));
+      cache.cap = cache.order.size();
     }
-    TRI_CUDA_TRY(cudaMemcpy(d_order, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    last_cells = cells;
+    TRI_CUDA_TRY(cudaMemcpy(cache.d_order, cache.order.data(), cache.order.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice));
+    cache.cells = std::move(cells);
   }
-  for (size_t w = 0; w + 1 < waves.size(); w++) {
-    const int off = waves[w], cnt = waves[w + 1] - off;
-    kr_extbc<<<nblocks(cnt), kThreads, 0, s>>>(d_order + off, cnt, nrows, ncols, dt, h, qx, qy, dem, n,
+  for (size_t w = 0; w + 1 < cache.waves.size(); w++) {
+    const int off = cache.waves[w], cnt = cache.waves[w + 1] - off;
+    kr_extbc<<<nblocks(cnt), kThreads, 0, s>>>(cache.d_order + off, cnt, nrows, ncols, dt, h, qx, qy, dem, n,
                                                 relative_index, extbctype, start_index, nrows_vars, extbcvar1,
                                                 extbcvar2, simtime, rank, total_process);
   }
@@ -576,6 +614,9 @@ extern "C" int tri_kernel_compute_extbc_values_noalloc_f64(
     build_waves(touch, slot.order_host, slot.waves);
     TRI_CUDA_TRY(cudaMemcpyAsync(slot.order, slot.order_host.data(), slot.order_host.size() * sizeof(int32_t),
                                  cudaMemcpyHostToDevice, s));
+    // The order is marked valid only once it has landed: a later call with
+    // the same list on another stream launches without copying it again.
+    TRI_CUDA_TRY(cudaStreamSynchronize(s));
     slot.cells = std::move(cells);
   }
   for (size_t w = 0; w + 1 < slot.waves.size(); w++) {

@@ -878,6 +878,19 @@ __device__ __forceinline__ void stage_abandon(DevClock* clk, uint64_t* bar, int 
   for (int g = from; g < kGroups; ++g) mbar_wait(&bar[g], 0);
 }
 
+// Test hook (one thread of one block): a bounded wait on a barrier whose
+// phase can never complete (its arrival count is met, but it expects 16 bytes
+// that no copy delivers, and no copy is ever issued on it).  The wait gives up
+// after clk->wait_test polls and records a device status as a stage timeout
+// does, so the host's handling of a wait that gave up can be tested without
+// disturbing any real copy.
+static __device__ __noinline__ void wait_test(DevClock* clk) {
+  __shared__ __align__(8) uint64_t bar;
+  mbar_init(&bar, 1);
+  mbar_arrive_expect_tx(&bar, 16);
+  if (!mbar_wait(&bar, 0, clk->wait_test)) atomicExch(&clk->status, kStatusTestWait);
+}
+
 template <typename T>
 __device__ __forceinline__ unsigned long long wetdry_staged(DevClock* __restrict__ clk, const StateBufs<T>& sb,
                                                             const BedMap<T>& bed, T* __restrict__ maxh, int rows,
@@ -1128,7 +1141,10 @@ __global__ void __launch_bounds__(kWetCols) k_wetdry_staged(DevClock* __restrict
   pdl_wait();
   pdl_trigger();
   if (!clk->active) return;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) fold_accounts(clk);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    fold_accounts(clk);
+    if (clk->wait_test) wait_test(clk);
+  }
   if (tzero != nullptr && *maxh_neg == 0 && band_all_zero<T>(clk, tzero, rows, cols, rb, blockIdx.x, blockIdx.y)) {
     if (threadIdx.x == 0) {  // interior cells of the skipped band
       const int ra = max((int)blockIdx.y * WetStage<T>::kBand, 1);

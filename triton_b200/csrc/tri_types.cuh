@@ -35,7 +35,7 @@ struct DevClock {
   int32_t nroff, roff_rows, nsrc, hyg_rows;
   int32_t status;  // nonzero: a device-side check failed (value = reason)
   uint32_t tile_next;  // work counter of the flux kernel's dynamic tiles, reset every step
-  uint32_t pad0;
+  uint32_t wait_test;  // test hook: nonzero = polls of a wait nothing completes (tri_domain_set_wait_test)
   unsigned long long dt_key[2];
   const double* roff_t;
   const double* hyg_t;

@@ -376,8 +376,12 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
     numeric = !cfg_arg.empty() && conv.eof() && !conv.fail();
   }
   if (!cfg_arg.empty() && !numeric) cfg_path = cfg_arg;
+  // The reference composes this path from the output folder before any cfg
+  // has been read, i.e. from an empty folder name (triton_init.h:98-101):
+  // <project>//cfg/config_<id>.cfg, not <project>/<output_folder>/cfg where
+  // the run wrote it; the rasters it then names come from <output_folder>.
   if (checkpoint_id > 0)
-    cfg_path = P.project_dir + "/output/cfg/config_" + std::to_string(checkpoint_id) + ".cfg";
+    cfg_path = P.project_dir + "//cfg/config_" + std::to_string(checkpoint_id) + ".cfg";
   P.cfg_content = read_file(cfg_path);
   Args& a = P.args;
   a = get_args(P.cfg_content);
@@ -460,11 +464,23 @@ Problem load_problem(const std::string& argv0, const std::string& cfg_arg, int c
       for (int j = 0; j < C; j++) rin[(size_t)(i + 1) * Cp + j + 1] = r[(size_t)i * C + j];
   }
   bool have_maxh = false;
-  if (a.checkpoint_id > 0) {  // checkpoint rasters (triton_init.h:303-353)
+  // Checkpoint rasters.  Sequential input reads <what>_<id>_00.out holding the
+  // whole domain, and only when output_option is SEQ (triton_init.h:303-353;
+  // otherwise the initial fields stand).  Partitioned input reads one file per
+  // rank, <what>_<id>_<rank>.out with that rank's rows (triton_init.h:577-626):
+  // files written by N ranks are stacked in rank order like the other
+  // partitioned rasters.
+  if (a.checkpoint_id > 0 && (par || a.output_option == "SEQ")) {
     const std::string t = two(a.checkpoint_id);
     const std::string base = P.project_dir + "/" + a.output_folder + "/bin/";
     auto hot = [&](const std::string& what) {
-      std::vector<double> v = pad(read_raster(base + what + "_" + t + "_00.out", R, C, false), R, C, 0.0);
+      std::vector<double> v =
+          pad(par ? read_parts<double>(base + what + "_" + t, ".out", R, C,
+                                       [](const std::string& path, int r, int c) {
+                                         return read_raster(path, r, c, false);
+                                       })
+                  : read_raster(base + what + "_" + t + "_00.out", R, C, false),
+              R, C, 0.0);
       if (a.open_boundaries) copy_ghosts(v, Rp, Cp);
       return v;
     };

@@ -407,6 +407,13 @@ int dump_problem(const char* argv0, const std::string& dir, const std::string& c
     << P.dem.xll << "\nyll " << P.dem.yll << "\ninit_dt " << P.init_dt << "\nrunoff_row " << P.runoff_row
     << "\nnroff " << P.nroff << "\nsimtime " << P.simtime << "\ncourant " << P.args.courant << "\nhextra "
     << P.args.hextra << "\n";
+  // the loop parameters of triton_simulate.h (as the run sets its clock)
+  const Args& a = P.args;
+  f << "sim_duration " << a.sim_duration << "\nprint_interval " << a.print_interval << "\nprint_observation "
+    << a.print_observation << "\ntime_series " << a.time_series_flag << "\nit_print " << a.it_print
+    << "\nit_count " << a.it_count << "\ntime_increment_fixed " << a.time_increment_fixed << "\ntime_step "
+    << a.time_step << "\nopen_boundaries " << a.open_boundaries << "\ncheckpoint_id " << a.checkpoint_id
+    << "\nnzones " << P.nroff << "\nroff_rows " << P.roff_rows << "\nhyg_rows " << P.hyg_rows << "\n";
   return 0;
 }
 
