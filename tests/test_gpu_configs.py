@@ -69,10 +69,13 @@ def test_thacker_2048_first_40s_matches_reference_executable(tmp_path):
 
 
 # Away from the shoreline: cells where the analytic depth is at least 0.5 m
-# (about 19 cells inland of the moving shoreline).  Bounds on the depth
-# error of this first-order scheme at dx = 4 m over the whole run:
-ANALYTIC_MAX = 0.05  # m
-ANALYTIC_RMS = 0.01  # m
+# (about 19 cells inland of the moving shoreline; 1.68 M cells).  Bounds on
+# the depth error of this first-order scheme at dx = 4 m over the whole run;
+# measured on a B200 (the FP64 path is deterministic): max 2.2e-3 m after a
+# quarter period growing to 5.5e-3 m after two periods, RMS 5.3e-4 m growing
+# to 1.9e-3 m (numerical damping of the 0.5 m oscillation).
+ANALYTIC_MAX = 0.01  # m
+ANALYTIC_RMS = 0.003  # m
 
 
 def test_thacker_2048_two_periods_against_analytic_solution():
