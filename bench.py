@@ -95,7 +95,7 @@ class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
@@ -136,8 +136,9 @@ class ClockSampler:
         load = [s for s in sm if s > 0.5 * smax] or sm
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        util = [float(r[9]) for r in rows if len(r) > 9 and r[9].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "util_mean": statistics.mean(util) / 100.0 if util else None}
 
 
 # ---------------------------------------------------------------------------
@@ -159,8 +160,9 @@ def cfl_dt0(sc):
     import numpy as np
     h, qx, qy = sc.h, sc.qx, sc.qy
     wet = h > sc.hextra
-    u = np.where(wet, np.maximum(abs(qx), abs(qy)) / np.where(wet, h, 1), 0)
-    dt = np.where(wet, sc.courant * sc.dx / (u + 3.132091953 * np.sqrt(np.where(wet, h, 0))), np.inf)
+    with np.errstate(divide="ignore"):
+        u = np.where(wet, np.maximum(abs(qx), abs(qy)) / np.where(wet, h, 1), 0)
+        dt = np.where(wet, sc.courant * sc.dx / (u + 3.132091953 * np.sqrt(np.where(wet, h, 0))), np.inf)
     return float(dt.min())
 
 
@@ -194,19 +196,49 @@ def run_reference(sc, steps, threads):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def host_cores():
+    """(physical cores, logical CPUs) this process may run on: distinct
+    (package, core) pairs of /proc/cpuinfo among the CPUs of its affinity."""
+    cpus = sorted(os.sched_getaffinity(0))
+    pairs, cur, phys = {}, None, "0"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "processor":
+                    cur = int(v)
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id" and cur is not None:
+                    pairs[cur] = (phys, v)
+    except OSError:
+        pass
+    cores = len({pairs[c] for c in cpus if c in pairs}) or len(cpus)
+    return cores, len(cpus)
+
+
+def workload_config(sc, desc, precision, world):
+    return {"workload": desc, "grid": [sc.rows - 2, sc.cols - 2], "interior_cells": sc.interior_cells,
+            "precision": precision, "parallelism": f"replicas x{world}" if world > 1 else "single"}
+
+
 def reference_arm(args, sc, desc):
-    threads = len(os.sched_getaffinity(0))
-    r = run_reference(sc, args.steps + args.warmup, threads)
+    cores, logical = host_cores()
+    r = run_reference(sc, args.steps, cores)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/triton_ref_omp was not built"}))
         return
     val, its, secs = r
+    cfg = workload_config(sc, desc, args.precision, 1)
+    cfg["engine"] = (f"reference TRITON sources, OpenMP build, {cores} threads (one per physical core of "
+                     f"{logical} logical CPUs)")
     line = {"metric": METRIC, "value": val, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": its,
             "warmup": 0, "ms_per_step": 1000.0 * secs / its, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "engine": "reference TRITON sources, OpenMP build, all host threads"},
-            "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
-                             "sample": f"{its} time steps of the workload ({secs:.2f} s compute)"},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "config": cfg,
+            "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"{its} time steps of the workload ({secs:.2f} s compute), "
+                                       f"{cores} OpenMP threads on {cores} physical cores"},
             "e2e": {"value": val, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -261,60 +293,174 @@ def _timed(stream, fn):
     return out, e0.elapsed_time(e1)
 
 
-def measure_forms(args, sc, stream, value64):
-    """The other forms on one GPU, after the headline measurement.
+def _form(out, name, fn):
+    """Runs one form; a failure is recorded in its entry instead of ending
+    the run (the headline line is printed either way)."""
+    t0 = time.perf_counter()
+    try:
+        out[name] = fn()
+    except Exception as e:  # noqa: BLE001
+        out[name] = {"error": f"{type(e).__name__}: {e}"[:500]}
+    out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
 
-    fp32: the same Thacker workload in the FP32 precision form.
-    ensemble: `--ens-members` watershed members (side log-uniform in
-    256..`--ens-max-side`, dx 5-20 m, rain 10-100 mm/h for 1 h, Manning
+
+def _domain_window(sc, prec, stream, spinup, steps, warmup):
+    """One domain of `sc` in `prec`, launch shape autotuned: `spinup` +
+    `warmup` untimed steps, `steps` timed with CUDA events at the two ends,
+    then the same number again with an event pair around every flux and
+    wet-dry launch for the per-kernel figures."""
+    d = sc.to_domain(prec, stream=stream.cuda_stream)
+    try:
+        d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+        tune = d.autotune(trial_steps=8)
+        d.advance(spinup + warmup)
+        (n, _), ms = _timed(stream, lambda: d.advance(steps))
+        d.set_timing(True)
+        d.advance(steps)
+        torch_sync()
+        flux_ms, flux_n, wet_ms, wet_n = d.get_timing()
+        fcells, _ = d.get_work()
+        d.set_timing(False)
+    finally:
+        d.close()
+    cells = sc.interior_cells
+    peak, kind = _peaks()
+    flux_s = flux_ms / max(flux_n, 1) / 1000.0
+    fl_cells = fcells / max(flux_n, 1)
+    step_gbs = ALG_BYTES_STEP[prec] * cells * n / (ms / 1000.0) / 1e9
+    return {"value": cells * n / (ms / 1000.0), "unit": "cell-updates/s", "ms_per_step": ms / n, "steps": n,
+            "flux_launch_shape": {k: tune[k] for k in ("variant", "rows_per_tile")},
+            "roofline": {"bound": "hbm", "kernel": "k_flux_update", "unit": "GB/s",
+                         "achieved": ALG_BYTES_FLUX[prec] * fl_cells / flux_s / 1e9, "peak": peak,
+                         "frac": ALG_BYTES_FLUX[prec] * fl_cells / flux_s / 1e9 / peak,
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({kind})",
+                         "computed_cell_frac": fl_cells / cells, "avg_launch_ms": flux_s * 1000.0,
+                         "wetdry_dt_avg_launch_ms": wet_ms / max(wet_n, 1), "step_achieved_gbs": step_gbs,
+                         "step_frac": step_gbs / peak}}
+
+
+def torch_sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def form_watershed(args, stream):
+    """The precision form's watershed (side --ws-n, 8192 by default: 67 M
+    cells, dx 10 m, fractal terrain 0-300 m with a carved valley, log-normal
+    Manning, 3 point inflows, rain 50 mm/h, open outflow on the lowest edge)
+    in FP64 and in FP32: a window of --ws-steps steps after 120 steps of
+    spin-up.  Rain falls on every cell, so every tile is computed (a domain
+    with runoff never skips dry tiles)."""
+    from triton_b200 import scenarios
+    sc = scenarios.watershed(n=args.ws_n, dx=10.0, seed=1234, gpu_noise=True)
+    out = {"workload": f"watershed {args.ws_n}x{args.ws_n}, dx 10 m, fractal DEM 0-300 m + carved valley, "
+                       "log-normal Manning (median 0.035, sigma 0.3), 3 inflows, rain 50 mm/h, open outflow "
+                       f"edge; {args.ws_steps} steps after 120 of spin-up, every tile computed",
+           "interior_cells": sc.interior_cells}
+    for prec in ("fp64", "fp32"):
+        out[prec] = _domain_window(sc, prec, stream, 120, args.ws_steps, args.warmup)
+    out["fp32_vs_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def form_ensemble(args, stream):
+    """--ens-members watershed members (side log-uniform in
+    256..--ens-max-side, dx 5-20 m, rain 10-100 mm/h for 1 h, Manning
     median +/-30 %, 3 h), advanced as one batch in FP32 and in FP64, and the
-    same members advanced one after another as plain FP64 domains; every
-    figure is interior cells x steps over CUDA-event time on one stream."""
+    same members one after another as plain FP64 domains; every figure is
+    interior cells x steps over CUDA-event time on one stream.  Members are
+    built one at a time straight into their domains."""
     from triton_b200 import scenarios
     from triton_b200.batch import Batch
-    out = {}
-    d = sc.to_domain("fp32", stream=stream.cuda_stream)
-    d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
-    tune32 = d.autotune(trial_steps=8)
-    d.advance(args.warmup)
-    (n, _), ms = _timed(stream, lambda: d.advance(args.steps))
-    d.close()
-    v32 = sc.interior_cells * n / (ms / 1000.0)
-    out["fp32"] = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms / n, "vs_fp64": v32 / value64,
-                   "flux_launch_shape": {k: tune32[k] for k in ("variant", "rows_per_tile")}}
-    if args.ens_members <= 0:
-        return out
-    members = scenarios.ensemble(members=args.ens_members, seed=2024, side_min=256, side_max=args.ens_max_side,
-                                 duration=3 * 3600.0, gpu_noise=True)
-    cells = sum(m.interior_cells for m in members)
-    ens = {"members": len(members), "interior_cells": cells, "batched_steps": args.ens_steps,
-           "workload": f"{len(members)} rain-on-grid watersheds, side log-uniform 256..{args.ens_max_side}, "
-                       "dx 5-20 m, rain 10-100 mm/h for 1 h, Manning median +/-30 %, 3 h"}
-    for prec in ("fp32", "fp64"):
-        doms = [m.to_domain(prec, stream=stream.cuda_stream) for m in members]
-        for dm in doms:
-            dm.set_clock(print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
-        b = Batch(doms, stream=stream.cuda_stream)
-        tune = b.autotune(3)
-        b.advance(args.warmup)
-        p, ms = _timed(stream, lambda: b.advance(args.ens_steps))
-        ens[f"{prec}_batched"] = p.cell_updates / (ms / 1000.0)
-        ens[f"{prec}_batched_shape"] = {k: tune[k] for k in ("variant", "rows_per_tile")}
-        b.close()
-        if prec == "fp64":  # the same members as plain FP64 runs, one after another
-            def solo():
-                u = 0
-                for dm, m in zip(doms, members):
-                    k, _ = dm.advance(args.ens_steps)
-                    u += k * m.interior_cells
-                return u
-            u, ms = _timed(stream, solo)
-            ens["fp64_sequential"] = u / (ms / 1000.0)
-        for dm in doms:
-            dm.close()
+    doms = {"fp32": [], "fp64": []}
+    cells = []
+    try:
+        for m in scenarios.ensemble_iter(members=args.ens_members, seed=2024, side_min=256,
+                                         side_max=args.ens_max_side, duration=3 * 3600.0, gpu_noise=True):
+            cells.append(m.interior_cells)
+            for prec, lst in doms.items():
+                dm = m.to_domain(prec, stream=stream.cuda_stream)
+                dm.set_clock(print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+                lst.append(dm)
+        ens = {"members": len(cells), "interior_cells": sum(cells), "batched_steps": args.ens_steps,
+               "workload": f"{len(cells)} rain-on-grid watersheds, side log-uniform 256..{args.ens_max_side}, "
+                           "dx 5-20 m, rain 10-100 mm/h for 1 h, Manning median +/-30 %, 3 h"}
+        for prec in ("fp32", "fp64"):
+            b = Batch(doms[prec], stream=stream.cuda_stream)
+            tune = b.autotune(3)
+            b.advance(args.warmup)
+            p, ms = _timed(stream, lambda: b.advance(args.ens_steps))
+            ens[f"{prec}_batched"] = p.cell_updates / (ms / 1000.0)
+            ens[f"{prec}_batched_ms_per_step"] = ms / args.ens_steps
+            ens[f"{prec}_batched_shape"] = {k: tune[k] for k in ("variant", "rows_per_tile")}
+            b.close()
+        def solo():  # the same members as plain FP64 runs, one after another
+            u = 0
+            for dm, c in zip(doms["fp64"], cells):
+                k, _ = dm.advance(args.ens_steps)
+                u += k * c
+            return u
+        u, ms = _timed(stream, solo)
+        ens["fp64_sequential"] = u / (ms / 1000.0)
+    finally:
+        for lst in doms.values():
+            for dm in lst:
+                dm.close()
     ens["fp32_batched_vs_fp64_batched"] = ens["fp32_batched"] / ens["fp64_batched"]
     ens["fp32_batched_vs_fp64_sequential"] = ens["fp32_batched"] / ens["fp64_sequential"]
-    out["ensemble"] = ens
+    return ens
+
+
+def form_serving(args):
+    """A short serving window below capacity: Poisson arrivals at
+    --form-serve-rate per s for --form-serve-seconds (the serving workload's
+    scenarios: side log-uniform 512..4096, 0.5-6 h simulated, 20 % FP64),
+    stopped after --form-serve-max-wall s; p50/p99 solve latency of the
+    completed requests, scenarios/hour, cell-updates/s and the GPU's busy
+    fraction (nvidia-smi utilization.gpu) over the window."""
+    from triton_b200.serving import Server, poisson_requests, summary
+    reqs = poisson_requests(rate=args.form_serve_rate, seconds=args.form_serve_seconds, seed=11)
+    srv = Server(hbm_budget=150e9, chunk_steps=32)
+    sampler = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+    sampler.start()
+    t0 = time.perf_counter()
+    srv.run(reqs, deadline=args.form_serve_max_wall)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    s = summary(reqs, wall)
+    return dict(s, workload=f"Poisson arrivals {args.form_serve_rate}/s for {args.form_serve_seconds:.0f} s, side "
+                            "log-uniform 512..4096, 0.5-6 h simulated, 20% FP64 / 80% FP32, 150 GB budget",
+                wall_limit_s=args.form_serve_max_wall, unfinished=sum(r.finished is None for r in reqs),
+                peak_hbm_used_bytes=srv.peak_used, cell_updates_per_s_all_work=srv.cell_updates / wall,
+                gpu_utilisation=(clocks or {}).get("util_mean"), clocks=clocks)
+
+
+def measure_forms(args, sc, stream, value64):
+    """The other forms on one GPU, after the headline measurement: the same
+    Thacker workload in FP32, the watershed window in both precisions, the
+    batched ensemble, and a short serving window."""
+    out = {}
+
+    def fp32():
+        d = sc.to_domain("fp32", stream=stream.cuda_stream)
+        try:
+            d.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0,
+                        time_series=0)
+            tune32 = d.autotune(trial_steps=8)
+            d.advance(args.warmup)
+            (n, _), ms = _timed(stream, lambda: d.advance(args.steps))
+        finally:
+            d.close()
+        v32 = sc.interior_cells * n / (ms / 1000.0)
+        return {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms / n, "vs_fp64": v32 / value64,
+                "flux_launch_shape": {k: tune32[k] for k in ("variant", "rows_per_tile")}}
+    _form(out, "fp32", fp32)
+    if args.ws_n > 0:
+        _form(out, "watershed", lambda: form_watershed(args, stream))
+    if args.ens_members > 0:
+        _form(out, "ensemble", lambda: form_ensemble(args, stream))
+    if args.form_serve_seconds > 0:
+        _form(out, "serving", lambda: form_serving(args))
     return out
 
 
@@ -361,10 +507,16 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="", help="flux kernel launch shape 'variant:rows_per_tile' (skips autotune)")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 and ensemble measurements")
-    ap.add_argument("--ens-members", type=int, default=64)
-    ap.add_argument("--ens-max-side", type=int, default=1024)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the other forms (FP32, watershed window, ensemble, serving window)")
+    ap.add_argument("--ws-n", type=int, default=8192, help="forms: watershed side (0: skip)")
+    ap.add_argument("--ws-steps", type=int, default=200, help="forms: watershed window steps")
+    ap.add_argument("--ens-members", type=int, default=256, help="forms: ensemble members (0: skip)")
+    ap.add_argument("--ens-max-side", type=int, default=2048)
     ap.add_argument("--ens-steps", type=int, default=100)
+    ap.add_argument("--form-serve-rate", type=float, default=0.15, help="forms: serving window arrival rate (1/s)")
+    ap.add_argument("--form-serve-seconds", type=float, default=60.0, help="forms: serving window (s; 0: skip)")
+    ap.add_argument("--form-serve-max-wall", type=float, default=150.0, help="forms: serving window wall limit (s)")
     ap.add_argument("--serve-seconds", type=float, default=600.0, help="serve: arrival window (s)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--serve-max-wall", type=float, default=0.0, help="serve: stop after this many s (0: window x 2)")
@@ -439,8 +591,10 @@ def main():
             for k in ("h", "qx", "qy", "z", "n2")}
     outs = {k: torch.empty(sc.rows * sc.cols, dtype=torch.float64).pin_memory() for k in ("h", "qx", "qy", "maxh")}
     d2 = sc.to_domain(args.precision, stream=stream.cuda_stream)
-    d2.set_clock(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    quiet = dict(sim_duration=1e300, print_interval=1e300, print_observation=1e300, it_print=0, time_series=0)
+    d2.set_clock(**quiet)
     d2.set_shape(tuning["variant"], tuning["rows_per_tile"])  # the launch shape the device-timed run used
+    d2.advance(args.warmup)  # a domain that has stepped before (its step graph exists), as a served one has
     import ctypes as C
 
     from triton_b200 import _abi
@@ -450,9 +604,12 @@ def main():
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
+    # a new job: terrain, roughness and initial state from host memory, max
+    # depth started from the initial depth on the device, the clock reset
     for k in ("z", "n2", "h", "qx", "qy"):
         _abi.check(L.tri_domain_upload(d2._h, fid[k], C.cast(host[k].data_ptr(), _abi._dp), sc.rows * sc.cols))
-    _abi.check(L.tri_domain_upload(d2._h, fid["maxh"], C.cast(host["h"].data_ptr(), _abi._dp), sc.rows * sc.cols))
+    _abi.check(L.tri_domain_init_max_depth(d2._h))
+    d2.set_clock(**dict(sc.clock(), **quiet))
     n2_, _ = d2.advance(args.steps)
     for k in ("h", "qx", "qy", "maxh"):
         _abi.check(L.tri_domain_download(d2._h, fid[k], C.cast(outs[k].data_ptr(), _abi._dp), sc.rows * sc.cols))
@@ -461,7 +618,7 @@ def main():
     barrier(world)
     ems = f0.elapsed_time(f1)
     e2e_val = cells * n2_ * world / (max_over_ranks(ems, world, "cuda") / 1000.0)
-    h2d = 6 * sc.rows * sc.cols * 8
+    h2d = 5 * sc.rows * sc.cols * 8
     d2h = 4 * sc.rows * sc.cols * 8
     d2.close()
 
@@ -477,11 +634,12 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = len(os.sched_getaffinity(0))
-        r = run_reference(sc, 60, threads)
+        cores, logical = host_cores()
+        r = run_reference(sc, 60, cores)
         if r is not None:
-            cpu = {"value": r[0], "unit": "cell-updates/s", "cores": threads, "kind": "reference",
-                   "sample": f"{r[1]} time steps of the same workload, reference OpenMP build ({r[2]:.2f} s compute)"}
+            cpu = {"value": r[0], "unit": "cell-updates/s", "cores": cores, "kind": "reference",
+                   "sample": f"{r[1]} time steps of the same workload, reference OpenMP build ({r[2]:.2f} s "
+                             f"compute), {cores} threads on {cores} physical cores ({logical} logical CPUs)"}
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms and args.precision == "fp64":
@@ -493,11 +651,10 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
             "data": "synthetic",
-            "config": {"workload": desc, "grid": [sc.rows - 2, sc.cols - 2], "interior_cells": cells,
-                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state ~%d MB per GPU)" % (
-                           sc.rows * sc.cols * (72 if args.precision == "fp64" else 36) // 2 ** 20),
-                       "flux_launch_shape": tuning},
+            "config": dict(workload_config(sc, desc, args.precision, world),
+                           l2="inputs larger than L2 (state ~%d MB per GPU)" % (
+                               sc.rows * sc.cols * (72 if args.precision == "fp64" else 36) // 2 ** 20),
+                           flux_launch_shape=tuning),
             "roofline": {"bound": "hbm", "kernel": "k_flux_update", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": (tpc * cells) if tpc is not None else None,

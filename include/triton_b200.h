@@ -129,6 +129,11 @@ int tri_domain_destroy(tri_domain* d);
  * H, QX or QY (or DEM) invalidates the cached CFL dt. */
 int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t n);
 int tri_domain_download(tri_domain* d, int32_t field, double* host, int64_t n);
+/* Max depth := the current depth, on the device (the reference starts its max
+ * depth array from the initial depth, triton_init.h:1239-1248, and copies it
+ * up with the rest): a caller without a max depth of its own saves one field
+ * of host-to-device traffic. */
+int tri_domain_init_max_depth(tri_domain* d);
 
 /* Forcing tables, flattened as in triton_init.h.
  *  runoff  (:1299-1357): zone id per padded cell (values in [0, nzones)),

@@ -65,6 +65,7 @@ _SIGS = {
     "tri_domain_destroy": (C.c_int, [_vp]),
     "tri_domain_upload": (C.c_int, [_vp, C.c_int32, _dp, C.c_int64]),
     "tri_domain_download": (C.c_int, [_vp, C.c_int32, _dp, C.c_int64]),
+    "tri_domain_init_max_depth": (C.c_int, [_vp]),
     "tri_domain_set_runoff": (C.c_int, [_vp, C.c_int32, C.c_int32, _dp, _dp, _ip, C.c_int64]),
     "tri_domain_set_sources": (C.c_int, [_vp, C.c_int32, _ip, C.c_int32, _dp, _dp]),
     "tri_domain_set_extbc": (C.c_int, [_vp, C.c_int32, _ip, _ip, _ip, _ip, C.c_int32, _dp, _dp]),

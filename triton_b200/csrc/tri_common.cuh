@@ -68,6 +68,23 @@ __device__ __forceinline__ float div_by_rcp<float>(float a, float, float y) {
   return a * y;
 }
 
+// div_by_rcp for a dividend that is never a zero (and never subnormal): with
+// q0 != 0, an exact quotient (r == 0) gives fma(0, y, q0) == q0, so the
+// zero-residual test is not needed.  The solver's uses: dt*p with |p| >=
+// 1e-12 (smaller face contributions are flushed to +0 before, and dt*(+0)
+// is the exact quotient +0 both ways: r = +0, fma(+0, y, +0) = +0), and
+// h*dx/2 with h > 0 (a depth, far above the subnormal range; the same
+// three operations as div_by_rcp there).
+template <typename T>
+__device__ __forceinline__ T div_nz(T a, T b, T y) {
+  const T q0 = a * y;
+  return dev_fma(dev_fma(-q0, b, a), y, q0);
+}
+template <>
+__device__ __forceinline__ float div_nz<float>(float a, float, float y) {
+  return a * y;
+}
+
 // a / b rounded to nearest for a divisor b shared by several quotients, from
 // y = RN(1/b): div_by_rcp where Markstein's conditions provably hold (|a| >=
 // 2^-900 so the residual a - b*q0 is exact, and q0 = RN(a*y) between 2^-1000
@@ -75,6 +92,9 @@ __device__ __forceinline__ float div_by_rcp<float>(float a, float, float y) {
 // dividend gives the signed zero of a/b.  Bit-identical to a / b for every
 // finite non-zero b; the solver divides by Roe-averaged celerities, sums of
 // sqrt(h) and the friction term this way.
+// (Tests of the same conditions on the 32-bit high words, with the zero
+// residual left to fma, measured 17 % slower on the FP64 flux kernel: the
+// code shape matters more than the instruction count here.)
 __device__ __forceinline__ double div_shared(double a, double b, double y) {
   const double q0 = a * y;
   const unsigned long long ba = (unsigned long long)__double_as_longlong(a);

@@ -307,10 +307,10 @@ void size_flux_grid(tri_domain* d) {
   d->flux_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + 3) / 4));
 }
 
-// Default shape before any tuning: the middle register budget (variant 1,
-// the fastest of the three on watersheds of 1024^2 to 8192^2) and the
-// largest tile height, 32 down to 8, that still gives every warp of a full
-// wave about eight tiles.
+// Default shape before any tuning: the register budget of 5 blocks per SM
+// in FP64 and 8 in FP32 (the fastest on watersheds of 1024^2 to 8192^2) and
+// the largest tile height, 32 down to 8, that still gives every warp of a
+// full wave about eight tiles.
 void choose_shape(tri_domain* d) {
   const int rows = d->desc.rows - 2, cols = d->desc.cols - 2;
   int sms = 148, dev = 0;
@@ -319,7 +319,7 @@ void choose_shape(tri_domain* d) {
   const int64_t warps = (int64_t)sms * 12;
   int rb = 32;
   while (rb > 8 && strips * ((rows + rb - 1) / rb) < 8 * warps) rb /= 2;
-  d->flux_variant = 1;
+  d->flux_variant = d->prec == TRI_FP64 ? 1 : 2;
   d->rb = rb;
   size_flux_grid(d);
 }
@@ -599,6 +599,26 @@ int tri_domain_upload(tri_domain* d, int32_t field, const double* host, int64_t 
     int rc2 = push_clock(d);
     if (rc2 != TRI_OK) return rc2;
   }
+  return TRI_OK;
+}
+
+int tri_domain_init_max_depth(tri_domain* d) {
+  TRI_CHECK_ARG(d, "null domain");
+  const size_t es = d->prec == TRI_FP64 ? 8 : 4;
+  const int64_t n = d->ncells;
+  void* h = d->h[d->mirror->cur];
+  TRI_CUDA_TRY(cudaMemcpyAsync(d->maxh, h, (size_t)n * es, cudaMemcpyDeviceToDevice, d->stream));
+  // dry bands skip the wet-dry kernel only while no max depth is negative
+  TRI_CUDA_TRY(cudaMemsetAsync(d->maxh_neg, 0, sizeof(int32_t), d->stream));
+  if (d->prec == TRI_FP64)
+    k_flag_negative<double><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const double*)d->maxh, n,
+                                                                                 d->maxh_neg);
+  else
+    k_flag_negative<float><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>((const float*)d->maxh, n,
+                                                                               d->maxh_neg);
+  TRI_CUDA_TRY(cudaGetLastError());
+  TRI_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->tz_dirty = true;
   return TRI_OK;
 }
 

@@ -64,7 +64,32 @@ struct FaceOut {
 template <typename T>
 struct StepK {
   T dx, dt, rdx, rdt, hextra;
+  bool dx_pow2;  // dx is a power of two: a / dx == a * rdx exactly (both round the same real)
 };
+
+// True for a positive normal power of two.
+__host__ __device__ inline bool is_pow2(double x) {
+  unsigned long long b;
+#ifdef __CUDA_ARCH__
+  b = (unsigned long long)__double_as_longlong(x);
+#else
+  __builtin_memcpy(&b, &x, 8);
+#endif
+  const unsigned long long e = b >> 52;
+  return (b & 0x000FFFFFFFFFFFFFull) == 0 && e >= 1 && e <= 0x7FE;
+}
+
+template <typename T>
+__host__ __device__ inline StepK<T> step_k(T dx, T dt, T rdx, T rdt, T hextra) {
+  StepK<T> K;
+  K.dx = dx;
+  K.dt = dt;
+  K.rdx = rdx;
+  K.rdt = rdt;
+  K.hextra = hextra;
+  K.dx_pow2 = is_pow2((double)dx);
+  return K;
+}
 
 // Products with the face normal (nx, ny) = (1,0) or (0,1): the component
 // itself (the product with the zero component is a zero term).
@@ -165,8 +190,8 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     // lam/(lam + lamE) is exactly 1 without an entropy-fix part (lam != 0 here)
     const T f0 = lamE2 == T(0) ? T(1) : lam0 / (lam0 + lamE2);
     const T f2 = lamE0 == T(0) ? T(1) : lam2 / (lam2 + lamE0);
-    be0 = dev_fmax(be0, f0 * (al0 * lam0 - div_by_rcp(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
-    be0 = dev_fmin(be0, f2 * (-al2 * lam2 + div_by_rcp(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
+    be0 = dev_fmax(be0, f0 * (al0 * lam0 - div_nz(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
+    be0 = dev_fmin(be0, f2 * (-al2 * lam2 + div_nz(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
   }
   const T be2 = -be0;
   const T be1 = T(0);
@@ -273,12 +298,23 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   if (dev_fabs(q1) < th1) q1 = T(0);
   if (dev_fabs(p2) < th1) p2 = T(0);
   if (dev_fabs(q2) < th1) q2 = T(0);
-  out.a0 = div_by_rcp(dt * p0, dx, K.rdx);
-  out.a1 = div_by_rcp(dt * p1, dx, K.rdx);
-  out.a2 = div_by_rcp(dt * p2, dx, K.rdx);
-  out.b0 = div_by_rcp(dt * q0, dx, K.rdx);
-  out.b1 = div_by_rcp(dt * q1, dx, K.rdx);
-  out.b2 = div_by_rcp(dt * q2, dx, K.rdx);
+  // rhs = dt*p/dx (kernels_flux.h:267-273); dt*p is +0 or at least dt*1e-12
+  if (K.dx_pow2) {  // uniform over the launch
+    const T s = K.rdx;
+    out.a0 = (dt * p0) * s;
+    out.a1 = (dt * p1) * s;
+    out.a2 = (dt * p2) * s;
+    out.b0 = (dt * q0) * s;
+    out.b1 = (dt * q1) * s;
+    out.b2 = (dt * q2) * s;
+  } else {
+    out.a0 = div_nz(dt * p0, dx, K.rdx);
+    out.a1 = div_nz(dt * p1, dx, K.rdx);
+    out.a2 = div_nz(dt * p2, dx, K.rdx);
+    out.b0 = div_nz(dt * q0, dx, K.rdx);
+    out.b1 = div_nz(dt * q1, dx, K.rdx);
+    out.b2 = div_nz(dt * q2, dx, K.rdx);
+  }
   return out;
 }
 

@@ -117,12 +117,7 @@ __global__ void kr_flux(int size, int nrows, int ncols, double dx, double dt, co
   a.sq = sqrth[id];  // the kernels read the SQRTH array, not sqrt(h)
   b.sq = sqrth[id2];
   const bool wet = (a.h > 0.0 || b.h > 0.0);
-  StepK<double> K;
-  K.dx = dx;
-  K.dt = dt;
-  K.rdx = 1.0 / dx;
-  K.rdt = 1.0 / dt;
-  K.hextra = hextra;
+  const StepK<double> K = step_k<double>(dx, dt, 1.0 / dx, 1.0 / dt, hextra);
   const FaceOut<double> f = face_flux<double, XFACE>(a, b, K);
   if (XFACE) {
     rhsh0[id] = f.a0;

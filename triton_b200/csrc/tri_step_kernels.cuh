@@ -128,11 +128,16 @@ static __global__ void k_clock(DevClock* __restrict__ c) {
 // Ghost cells are copied from the source to the destination buffer so both
 // ping-pong buffers keep the boundary state the reference keeps in place.
 // ---------------------------------------------------------------------------
+// rhs contributions collected for one cell before its south face is known.
+// The owner parts of its east and north faces are summed at once, in the
+// reference's order (flux_x writes rhs*0, flux_y adds to it):
+// r = e + n; the west face's neighbour part w waits for the south face's s
+// (rhs*1 = w + s).  Six values carried per lane instead of nine.
 template <typename T>
-struct RowParts {  // rhs contributions collected for one cell
-  T e0, e1, e2;    // east face, owner part   (flux_x rhs*0)
-  T w0, w1, w2;    // west face, neighbour part (flux_x rhs*1)
-  T n0, n1, n2;    // north face, owner part  (flux_y rhs*0)
+struct RowParts {
+  T r0, r1, r2;  // east + north owner parts
+  T w0, w1, w2;  // west face, neighbour part (flux_x rhs*1)
+  T an;          // FP32 form: |e0| + |n0|, for the noise test of the depth update
 };
 
 template <typename T>
@@ -143,8 +148,8 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
   const T hn = c.h;
   T hij;
   if (sizeof(T) == 8) {
-    const T rh0 = p.e0 + p.n0, rh1 = p.w0 + s0;
-    hij = hn - rh0 - rh1;
+    const T rh1 = p.w0 + s0;
+    hij = hn - p.r0 - rh1;
     clip = hij < T(0) ? -(double)hij : 0.0;
   } else {
     // FP32 form: the depth change is summed in FP64 and rounded
@@ -155,10 +160,10 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     // result within the rounding noise of its terms is zero, as FP32
     // arithmetic would give it: noise must not leave water on a cell that
     // drained, or the cell counts as wet.
-    const float parts = (p.e0 + p.n0) + (p.w0 + s0);
+    const float parts = p.r0 + (p.w0 + s0);
     float lo;
     const float hs = sr_add(hn, -parts, rnd, &lo);
-    const float noise = float(kNoise32) * (hn + dev_fabs(p.e0) + dev_fabs(p.n0) + dev_fabs(p.w0) + dev_fabs(s0));
+    const float noise = float(kNoise32) * (hn + p.an + dev_fabs(p.w0) + dev_fabs(s0));
     if (__fadd_rn(hn, -parts) <= noise) {
       clip = -((double)__fadd_rn(hn, -parts) + (double)lo);  // removed (noise) or clipped to zero: accounted
       hij = T(0);
@@ -173,10 +178,10 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     qxij = T(0);
     qyij = T(0);
   } else {
-    const T rx0 = p.e1 + p.n1, rx1 = p.w1 + s1;
-    const T ry0 = p.e2 + p.n2, ry1 = p.w2 + s2;
-    const T mx = c.qx - rx0 - rx1;
-    const T my = c.qy - ry0 - ry1;
+    const T rx1 = p.w1 + s1;
+    const T ry1 = p.w2 + s2;
+    const T mx = c.qx - p.r1 - rx1;
+    const T my = c.qy - p.r2 - ry1;
     const T modM = dev_sqrt(mx * mx + my * my);
     if (n2v > E12 && hn >= hextra && modM > E12) {
       const T tt = fdiv(dt * G * n2v * modM, hn * hn * dev_cbrt(hn));
@@ -257,11 +262,7 @@ __device__ __forceinline__ FluxCtx<T> flux_ctx(DevClock* clk, const StateBufs<T>
   X.roff_rows = clk->roff_rows;
   X.roff_row = clk->runoff_row;
   X.step = (uint32_t)clk->it_count;
-  X.K.dx = dx;
-  X.K.dt = T(clk->global_dt);
-  X.K.rdx = rdx;
-  X.K.rdt = T(clk->rdt);
-  X.K.hextra = hextra;
+  X.K = step_k<T>(dx, T(clk->global_dt), rdx, T(clk->rdt), hextra);
   X.tz_src = nullptr;
   X.tz_dst = nullptr;
   X.tpin = nullptr;
@@ -353,7 +354,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   if (r0 - 1 == 0 && owner) copy_ghost(0);
   fetch(r0);
   RowParts<T> pp;
-  pp.e0 = pp.e1 = pp.e2 = pp.w0 = pp.w1 = pp.w2 = pp.n0 = pp.n1 = pp.n2 = T(0);
+  pp.r0 = pp.r1 = pp.r2 = pp.w0 = pp.w1 = pp.w2 = pp.an = T(0);
   T pn2 = T(0);  // Manning of the previous row's cell
 
   for (int r = r0; r <= r1 + 1; ++r) {
@@ -373,14 +374,9 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn, clip,
                      cell_hash((uint32_t)id, 2u * X.step));
       if (kAcct) {
-        // Inflow through faces shared with ghost cells, in depth units.  The
-        // update is in fluctuation form, so the mass flux through a face of
-        // boundary cell i is F(Q_i).n plus the fluctuation it receives there:
-        // west / south faces dt/dx*q - b, east / north faces -(a + dt/dx*q).
-        // Also the depth the update clipped back to zero.
-        if (c == 1) acc_b += sxq * (double)prev.qx - (double)pp.w0;
-        if (c == cols - 2) acc_b -= (double)pp.e0 + sxq * (double)prev.qx;
-        if (r - 1 == 1) acc_b -= (double)pp.n0 + sxq * (double)prev.qy;
+        // Inflow through the south face of a cell of the last interior row
+        // (the other boundary faces are counted where their parts are
+        // formed, below), and the depth the update clipped back to zero.
         if (r - 1 == rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
         acc_c += clip;
       }
@@ -426,15 +422,23 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
     FaceOut<T> Xf;
     Xf.a0 = Xf.a1 = Xf.a2 = Xf.b0 = Xf.b1 = Xf.b2 = T(0);
     if (lane >= 1 && incol && c >= 1) Xf = face_flux<T, true>(left, cur, X.K);
-    pp.e0 = shfl_down1(Xf.a0);
-    pp.e1 = shfl_down1(Xf.a1);
-    pp.e2 = shfl_down1(Xf.a2);
+    const T e0 = shfl_down1(Xf.a0), e1 = shfl_down1(Xf.a1), e2 = shfl_down1(Xf.a2);
+    if (kAcct && upd) {
+      // Inflow through faces shared with ghost cells, in depth units.  The
+      // update is in fluctuation form, so the mass flux through a face of
+      // boundary cell i is F(Q_i).n plus the fluctuation it receives there:
+      // west / south faces dt/dx*q - b, east / north faces -(a + dt/dx*q).
+      if (c == 1) acc_b += sxq * (double)cur.qx - (double)Xf.b0;
+      if (c == cols - 2) acc_b -= (double)e0 + sxq * (double)cur.qx;
+      if (r == 1) acc_b -= (double)Y.a0 + sxq * (double)cur.qy;
+    }
+    pp.r0 = e0 + Y.a0;
+    pp.r1 = e1 + Y.a1;
+    pp.r2 = e2 + Y.a2;
     pp.w0 = Xf.b0;
     pp.w1 = Xf.b1;
     pp.w2 = Xf.b2;
-    pp.n0 = Y.a0;
-    pp.n1 = Y.a1;
-    pp.n2 = Y.a2;
+    if (sizeof(T) == 4) pp.an = dev_fabs(e0) + dev_fabs(Y.a0);
     pn2 = cn2;
     if (gcol) copy_ghost(r);
     prev = cur;

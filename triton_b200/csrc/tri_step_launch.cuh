@@ -30,13 +30,31 @@ StateBufs<T> bufs_of(const StepArgs& a) {
   return s;
 }
 
+// The flux kernel instance of a register-budget variant.
+template <typename T, bool SKIP>
+auto flux_kernel(int variant) -> decltype(&k_flux_update<T, FluxBudget<T>::v0, SKIP>) {
+  switch (variant) {
+    case 0: return &k_flux_update<T, FluxBudget<T>::v0, SKIP>;
+    case 1: return &k_flux_update<T, FluxBudget<T>::v1, SKIP>;
+    case 2: return &k_flux_update<T, FluxBudget<T>::v2, SKIP>;
+    case 3: return &k_flux_update<T, FluxBudget<T>::v3, SKIP>;
+    default: return &k_flux_update<T, FluxBudget<T>::v4, SKIP>;
+  }
+}
+template <typename T>
+auto batch_flux_kernel(int variant) -> decltype(&k_batch_flux<T, FluxBudget<T>::v0>) {
+  switch (variant) {
+    case 0: return &k_batch_flux<T, FluxBudget<T>::v0>;
+    case 1: return &k_batch_flux<T, FluxBudget<T>::v1>;
+    case 2: return &k_batch_flux<T, FluxBudget<T>::v2>;
+    case 3: return &k_batch_flux<T, FluxBudget<T>::v3>;
+    default: return &k_batch_flux<T, FluxBudget<T>::v4>;
+  }
+}
+
 template <typename T>
 void flux_occupancy(int variant, int* per_sm) {
-  switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v0, false>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v1, false>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_flux_update<T, FluxBudget<T>::v2, false>, 128, 0); break;
-  }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, flux_kernel<T, false>(variant), 128, 0);
 }
 
 // Launches kernel k after the previous work on stream s with programmatic
@@ -65,24 +83,12 @@ int launch_step(const StepArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   const BedMap<T> bed = bed_of<T>(a);
   TRI_CUDA_TRY(launch_pdl(k_clock, 1, 32, 0, s, a.clk));
   if (ev) cudaEventRecord(ev[0], s);
-#define TRI_FLUX_ARGS a.clk, sb, bed, (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero
-#define TRI_FLUX(V, SKIP) TRI_CUDA_TRY(launch_pdl(k_flux_update<T, FluxBudget<T>::V, SKIP>, a.flux_blocks, 128, 0, s, \
-                                                 TRI_FLUX_ARGS))
-  if (a.tzero != nullptr) {  // dry-tile skipping
-    switch (a.flux_variant) {
-      case 0: TRI_FLUX(v0, true); break;
-      case 1: TRI_FLUX(v1, true); break;
-      default: TRI_FLUX(v2, true); break;
-    }
-  } else {
-    switch (a.flux_variant) {
-      case 0: TRI_FLUX(v0, false); break;
-      case 1: TRI_FLUX(v1, false); break;
-      default: TRI_FLUX(v2, false); break;
-    }
-  }
-#undef TRI_FLUX
-#undef TRI_FLUX_ARGS
+  if (a.tzero != nullptr)  // dry-tile skipping
+    TRI_CUDA_TRY(launch_pdl(flux_kernel<T, true>(a.flux_variant), a.flux_blocks, 128, 0, s, a.clk, sb, bed,
+                            (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero));
+  else
+    TRI_CUDA_TRY(launch_pdl(flux_kernel<T, false>(a.flux_variant), a.flux_blocks, 128, 0, s, a.clk, sb, bed,
+                            (const T*)a.n2, a.zone, (const T*)a.rates, rows, cols, a.rb, dx, rdx, hx, a.tzero));
   if (ev) cudaEventRecord(ev[1], s);
   for (int w = 0; a.nsrc > 0 && w < a.n_src_waves; w++) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
@@ -119,22 +125,14 @@ int launch_initial_dt(const StepArgs& a, cudaStream_t s) {
 
 template <typename T>
 void batch_flux_occupancy(int variant, int* per_sm) {
-  switch (variant) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v0>, 128, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v1>, 128, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_flux<T, FluxBudget<T>::v2>, 128, 0); break;
-  }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, batch_flux_kernel<T>(variant), 128, 0);
 }
 
 template <typename T>
 int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
   const MemberDev<T>* mem = (const MemberDev<T>*)a.mem;
   k_batch_clock<T><<<(a.nm + 127) / 128, 128, 0, s>>>(mem, a.nm, a.ctl);
-  switch (a.flux_variant) {
-    case 0: k_batch_flux<T, FluxBudget<T>::v0><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
-    case 1: k_batch_flux<T, FluxBudget<T>::v1><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
-    default: k_batch_flux<T, FluxBudget<T>::v2><<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles); break;
-  }
+  batch_flux_kernel<T>(a.flux_variant)<<<a.flux_blocks, 128, 0, s>>>(mem, a.tile_member, a.ctl, a.ntiles);
   for (int w = 0; w < a.n_src_waves; w++) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
     k_batch_sources<T><<<(cnt + 127) / 128, 128, 0, s>>>(mem, a.src_items + off, cnt);

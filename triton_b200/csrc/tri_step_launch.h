@@ -13,26 +13,26 @@
 namespace tri {
 
 constexpr int kStripCols = 30;   // interior columns per warp tile of the flux kernel
-constexpr int kFluxVariants = 3; // register budgets (FluxBudget)
+constexpr int kFluxVariants = 5; // register budgets (FluxBudget)
 constexpr int kWetCols = 128;    // columns per block of the wet-dry/dt kernel
 constexpr int kWetBand = 16;     // rows per block of the initial-dt kernel
-// Blocks per SM that the flux kernel's three register-budget variants are
-// compiled for (__launch_bounds__ minimum).  FP64: 124, 96 and 80 registers a
-// thread (the last two spill a little to L1); FP32: 88, 64 and 48.  The
-// kernel is latency bound, so occupancy pays for the spills up to the middle
-// variant on single domains (8192^2 watershed, FP64: 4.57 ms a step with 5
-// blocks against 5.64 with 3); batches of small members run best on the
-// first (FP32: 22.2 G cell-updates/s with 5 blocks against 20.2 with 6).
+// Blocks of 128 threads per SM that the flux kernel's register-budget
+// variants are compiled for (__launch_bounds__ minimum).  FP64: 122, 96, 80,
+// 72 and 64 registers a thread (from 96 down they spill to L1, 8 to 300
+// bytes); FP32: 88, 80, 64, 48 and 40.  The kernel is latency bound, so
+// occupancy can pay for some spilling; the autotuner picks per domain.
 template <typename T>
 struct FluxBudget;
 template <>
 struct FluxBudget<double> {
-  static constexpr int v0 = 4, v1 = 5, v2 = 6;
+  static constexpr int v0 = 4, v1 = 5, v2 = 6, v3 = 7, v4 = 8;
 };
 template <>
 struct FluxBudget<float> {
-  static constexpr int v0 = 5, v1 = 8, v2 = 10;
+  static constexpr int v0 = 5, v1 = 6, v2 = 8, v3 = 10, v4 = 12;
 };
+// the variant untuned domains and batches start from
+constexpr int kFluxDefaultVariant = 1;
 // rows per block of the staged wet-dry/dt kernel (its shared-memory tile),
 // and output rows per group of its copies (each group on its own mbarrier)
 template <typename T>

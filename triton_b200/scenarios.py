@@ -280,8 +280,16 @@ def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0,
     a cell size in dx_range, a rain intensity in rain_range (mm/h) for
     rain_hours, the Manning median 0.035 perturbed uniformly by
     +/- manning_spread (relative) and its own terrain seed.  Members carry no point sources."""
+    return list(ensemble_iter(members, seed, side_min, side_max, dx_range, duration, rain_range, rain_hours,
+                              manning_spread, max_side, gpu_noise))
+
+
+def ensemble_iter(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0, 20.0),
+                  duration=3 * 3600.0, rain_range=(10.0, 100.0), rain_hours=1.0, manning_spread=0.3, max_side=None,
+                  gpu_noise=False):
+    """The members of ensemble(), built one at a time (a caller that loads
+    each into a domain holds one member's host arrays at a time)."""
     rng = np.random.default_rng(seed)
-    out = []
     for i in range(members):
         side = int(np.exp(rng.uniform(np.log(side_min), np.log(side_max))))
         if max_side is not None:
@@ -292,8 +300,7 @@ def ensemble(members=256, seed=2024, side_min=256, side_max=2048, dx_range=(5.0,
         sc = watershed(n=side, dx=dx, seed=int(rng.integers(1 << 31)), duration=duration, rain_mm_h=rain,
                        rain_hours=rain_hours, manning_median=mann, nsrc=0, gpu_noise=gpu_noise)
         sc.name = f"member{i:03d}"
-        out.append(sc)
-    return out
+        yield sc
 
 
 def extbc_segments(sc, segments):
