@@ -134,14 +134,16 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
     T e1 = un1 - SG * sqh1;
     T e2 = un2 - SG * sqh2;
     if (e1 < T(0) && e2 > T(0)) {
-      lamE0 = lam0 - e1 * (e2 - lam0) / (e2 - e1);
-      lam0 = e1 * (e2 - lam0) / (e2 - e1);
+      const T t = div_rare(e1 * (e2 - lam0), e2 - e1);
+      lamE0 = lam0 - t;
+      lam0 = t;
     }
     e1 = un1 + SG * sqh1;
     e2 = un2 + SG * sqh2;
     if (e1 < T(0) && e2 > T(0)) {
-      lamE2 = lam2 - e2 * (lam2 - e1) / (e2 - e1);
-      lam2 = e2 * (lam2 - e1) / (e2 - e1);
+      const T t = div_rare(e2 * (lam2 - e1), e2 - e1);
+      lamE2 = lam2 - t;
+      lam2 = t;
     }
   }
 
@@ -188,8 +190,8 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   hp = h1 + al0;
   if (lam0 * lam2 < T(0) && hp > T(0) && h1 > T(0) && h2 > T(0)) {
     // lam/(lam + lamE) is exactly 1 without an entropy-fix part (lam != 0 here)
-    const T f0 = lamE2 == T(0) ? T(1) : lam0 / (lam0 + lamE2);
-    const T f2 = lamE0 == T(0) ? T(1) : lam2 / (lam2 + lamE0);
+    const T f0 = lamE2 == T(0) ? T(1) : div_rare(lam0, lam0 + lamE2);
+    const T f2 = lamE0 == T(0) ? T(1) : div_rare(lam2, lam2 + lamE0);
     be0 = dev_fmax(be0, f0 * (al0 * lam0 - div_nz(h1 * dx * T(0.5), dt, K.rdt) + lamE2 * h2));
     be0 = dev_fmin(be0, f2 * (-al2 * lam2 + div_nz(h2 * dx * T(0.5), dt, K.rdt) + lamE0 * h1));
   }
@@ -200,9 +202,9 @@ __device__ __forceinline__ FaceOut<T> face_flux(const CellQ<T>& c1, const CellQ<
   // they only matter next to a dry cell, so they are formed only there
   T p0 = T(0), p1 = T(0), p2 = T(0);  // owner side
   T q0 = T(0), q1 = T(0), q2 = T(0);  // neighbour side
-  if (h2 < E12 && hp + be2 / lam2 < -E12) {
+  if (h2 < E12 && hp + div_rare(be2, lam2) < -E12) {
     p0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
-  } else if (h1 < E12 && hp - be0 / lam0 < -E12) {
+  } else if (h1 < E12 && hp - div_rare(be0, lam0) < -E12) {
     q0 += (lam0 * al0 - be0) + (lam2 * al2 - be2);
   } else {
     // wave 0: eigenvector (1, r01, r02)
