@@ -186,9 +186,21 @@ __device__ __forceinline__ void update_cell(const CellQ<T>& c, const RowParts<T>
     if (n2v > E12 && hn >= hextra && modM > E12) {
       const T tt = fdiv(dt * G * n2v * modM, hn * hn * dev_cbrt(hn));
       const T sq = dev_sqrt(T(1) + T(4) * tt);
-      const T rtt = recip(tt);
-      qxij = div_shared(T(-0.5) * (mx - mx * sq), tt, rtt);
-      qyij = div_shared(T(-0.5) * (my - my * sq), tt, rtt);
+      if (sizeof(T) == 8) {  // the reference's expression (kernels_state.h:86-96), bit for bit
+        const T rtt = recip(tt);
+        qxij = div_shared(T(-0.5) * (mx - mx * sq), tt, rtt);
+        qyij = div_shared(T(-0.5) * (my - my * sq), tt, rtt);
+      } else {
+        // FP32 form: -(m - m*s)/(2t) with s = sqrt(1 + 4t) equals
+        // 2m/(1 + s), without the cancellation of 1 - s: where t is small
+        // (deep, fast channel flow) 1 - s keeps only a few FP32 bits, and the
+        // rounding of s alone moved the friction-corrected discharge by up to
+        // 1e-3 of itself each step, one way (the 512^2 6 h watershed then
+        // ponded up to 0.97 m away from the FP64 run).
+        const T k = recip(T(1) + sq);
+        qxij = T(2) * mx * k;
+        qyij = T(2) * my * k;
+      }
     } else {
       qxij = mx;
       qyij = my;
