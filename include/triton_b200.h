@@ -232,8 +232,8 @@ int tri_selftest_division(int64_t n, uint64_t seed, int64_t* mismatches);
  * covers all members, the flux kernel taking tiles from a single queue over
  * all members.  Members stay tri_domain objects: upload, download, forcing,
  * observe and set_clock work on them between batch advances.  Members must
- * share one precision and have open_boundaries = 0.  A member whose forcing
- * changes after tri_batch_create needs a new batch. */
+ * share one precision; closed, open and external-boundary edges all batch.
+ * A member whose forcing changes after tri_batch_create needs a new batch. */
 typedef struct tri_batch tri_batch;
 typedef struct tri_batch_progress {
   int32_t steps;               /* most steps any member took */

@@ -20,7 +20,10 @@ def _members():
         sc.it_print = 37 + i
     mx = scenarios.mixed(rows=37, cols=53, seed=5)
     mx.name = "mixed"
-    return ms + [mx]
+    # open edges (zero-gradient ghosts, kernels.h:437-512) with sources and runoff
+    op = scenarios.mixed(rows=29, cols=44, seed=8, open_boundaries=1, with_extbc=False)
+    op.name = "open"
+    return ms + [mx, op]
 
 
 def _solo(sc, precision):

@@ -39,6 +39,8 @@ struct tri_batch {
   std::vector<int32_t> src_waves;
   int2* d_bc_items = nullptr;
   std::vector<int32_t> bc_waves;
+  int32_t* d_open = nullptr;  // members with open edges
+  int n_open = 0, open_dim = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   double tuned_ms = 0;
@@ -170,7 +172,25 @@ int build_items(tri_batch* b) {
   };
   int rc = gather(true, &b->d_src_items, b->src_waves);
   if (rc == TRI_OK) rc = gather(false, &b->d_bc_items, b->bc_waves);
-  return rc;
+  if (rc != TRI_OK) return rc;
+  // open-boundary members: ghost copies after the sources, before the
+  // external-boundary cells, as in the single-domain step
+  std::vector<int32_t> open;
+  b->open_dim = 0;
+  for (size_t m = 0; m < b->members.size(); m++) {
+    const tri_grid_desc& g = b->members[m]->desc;
+    if (!g.open_boundaries) continue;
+    open.push_back((int32_t)m);
+    b->open_dim = std::max(b->open_dim, std::max(g.rows, g.cols));
+  }
+  if (b->d_open) cudaFree(b->d_open);
+  b->d_open = nullptr;
+  b->n_open = (int)open.size();
+  if (!open.empty()) {
+    TRI_CUDA_TRY(cudaMalloc((void**)&b->d_open, open.size() * sizeof(int32_t)));
+    TRI_CUDA_TRY(cudaMemcpy(b->d_open, open.data(), open.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  return TRI_OK;
 }
 
 BatchArgs batch_args(tri_batch* b) {
@@ -190,6 +210,9 @@ BatchArgs batch_args(tri_batch* b) {
   a.bc_items = b->d_bc_items;
   a.bc_waves = b->bc_waves.data();
   a.n_bc_waves = (int)b->bc_waves.size() - 1;
+  a.open_members = b->d_open;
+  a.n_open = b->n_open;
+  a.open_dim = b->open_dim;
   return a;
 }
 
@@ -287,16 +310,13 @@ int reset_ctl(tri_batch* b) {
   return TRI_OK;
 }
 
-// Members of one batch: existing, distinct, one precision, no open edges.
+// Members of one batch: existing, distinct, one precision.
 int check_members(int prec, int32_t n, tri_domain* const* members, std::vector<tri_domain*>& out) {
   out.clear();
   for (int i = 0; i < n; i++) {
     tri_domain* d = members[i];
-    if (!d || d->prec != prec || d->desc.open_boundaries)
-      return set_error(TRI_E_INVALID,
-                       "batch member %d: members must exist, share one precision and use closed or "
-                       "external-boundary edges (open_boundaries=0)",
-                       i);
+    if (!d || d->prec != prec)
+      return set_error(TRI_E_INVALID, "batch member %d: members must exist and share one precision", i);
     for (int j = 0; j < i; j++)
       if (members[j] == d) return set_error(TRI_E_INVALID, "batch member %d repeats member %d", i, j);
     out.push_back(d);
@@ -358,6 +378,7 @@ int tri_batch_destroy(tri_batch* b) {
   if (b->h_seen) cudaFreeHost(b->h_seen);
   if (b->d_src_items) cudaFree(b->d_src_items);
   if (b->d_bc_items) cudaFree(b->d_bc_items);
+  if (b->d_open) cudaFree(b->d_open);
   for (int i = 0; i < 2; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

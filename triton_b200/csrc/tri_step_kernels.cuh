@@ -546,20 +546,17 @@ __global__ void k_sources(DevClock* __restrict__ clk, StateBufs<T> sb, const int
   atomicAdd(&clk->acc_step[kAccSources], (double)hs);
 }
 
+// Final values of copy_info_to_exterior_boundaries_west_east followed by
+// _north_south (kernels.h:437-512), item k of max(rows, cols): ghost columns
+// take the adjacent interior column (rows 1..rows-2), ghost rows take the
+// adjacent interior row, corners the diagonal interior cell.
 template <typename T>
-__global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows, int cols) {
-  pdl_wait();
-  pdl_trigger();
-  if (!clk->active) return;
+__device__ __forceinline__ void open_bc_item(const DevClock* __restrict__ clk, const StateBufs<T>& sb, int rows,
+                                             int cols, int k) {
   const int d = clk->dst;
   T* h = sb.H(d);
   T* qx = sb.QX(d);
   T* qy = sb.QY(d);
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  // Final values of copy_info_to_exterior_boundaries_west_east followed by
-  // _north_south: ghost columns take the adjacent interior column (rows
-  // 1..rows-2), ghost rows take the adjacent interior row, corners the
-  // diagonal interior cell.
   auto cp = [&](size_t g, size_t i) {
     h[g] = h[i];
     qx[g] = qx[i];
@@ -578,6 +575,14 @@ __global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int
     cp((size_t)cc, (size_t)cols + ci);
     cp((size_t)(rows - 1) * cols + cc, (size_t)(rows - 2) * cols + ci);
   }
+}
+
+template <typename T>
+__global__ void k_open_bc(const DevClock* __restrict__ clk, StateBufs<T> sb, int rows, int cols) {
+  pdl_wait();
+  pdl_trigger();
+  if (!clk->active) return;
+  open_bc_item<T>(clk, sb, rows, cols, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // compute_extbc_values for one boundary cell (kernels.h:254-420), single rank.
@@ -1222,6 +1227,15 @@ __global__ void __launch_bounds__(kWetCols) k_batch_wetdry(const MemberDev<T>* _
       wetdry_staged<T>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, M.hextra, M.arrival, M.arrival_depth,
                        (int)(local % M.wet_nbx), (int)(local / M.wet_nbx), reinterpret_cast<T*>(wet_smem));
   block_min_into(key, &clk->dt_key[clk->wr]);
+}
+
+// Open-boundary ghosts of the batch members that have open edges: block row
+// y serves member open_members[y].
+template <typename T>
+__global__ void k_batch_open_bc(const MemberDev<T>* __restrict__ mem, const int32_t* __restrict__ open_members) {
+  const MemberDev<T>& M = mem[open_members[blockIdx.y]];
+  if (!M.clk->active) return;
+  open_bc_item<T>(M.clk, M.sb, M.rows, M.cols, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Sparse forcing of a batch: items are (member, index) pairs of one

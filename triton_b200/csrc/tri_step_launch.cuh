@@ -137,6 +137,9 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
     const int off = a.src_waves[w], cnt = a.src_waves[w + 1] - off;
     k_batch_sources<T><<<(cnt + 127) / 128, 128, 0, s>>>(mem, a.src_items + off, cnt);
   }
+  if (a.n_open > 0)
+    k_batch_open_bc<T><<<dim3((unsigned)((a.open_dim + 255) / 256), (unsigned)a.n_open), 256, 0, s>>>(
+        mem, a.open_members);
   for (int w = 0; w < a.n_bc_waves; w++) {
     const int off = a.bc_waves[w], cnt = a.bc_waves[w + 1] - off;
     k_batch_extbc<T><<<(cnt + 127) / 128, 128, 0, s>>>(mem, a.bc_items + off, cnt);

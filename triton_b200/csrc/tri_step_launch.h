@@ -105,6 +105,8 @@ struct BatchArgs {
   const int2* bc_items;
   const int32_t* bc_waves;
   int n_bc_waves;
+  const int32_t* open_members;  // members with open edges (device), their count and largest max(rows, cols)
+  int n_open, open_dim;
 };
 template <typename T>
 int launch_batch_step(const BatchArgs& a, cudaStream_t s);
