@@ -262,6 +262,18 @@ int tri_batch_wait(tri_batch* b, tri_batch_progress* out);
 /* Launch-shape autotuner of the batched flux kernel; members' states, maximum
  * depths and clocks are restored afterwards. */
 int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out);
+/* How batched steps are launched (no reference counterpart).
+ * TRI_BATCH_GRAPHS (default): per batched step one launch per kernel type
+ * (clock, flux, forcing waves, wet-dry/dt), 8 steps captured as a CUDA graph.
+ * TRI_BATCH_SINGLE_LAUNCH: one persistent launch runs up to 32 batched
+ * steps; its blocks take work items (a member's clock, four flux tiles, a
+ * member's forcing, a wet-dry block) in a fixed order and each item waits,
+ * bounded, only for the items of its own member it depends on, so members
+ * advance without any grid-wide barrier.  Both compute exactly what every
+ * member computes alone.  A dependency wait that gives up makes the advance
+ * return TRI_E_TIMEOUT. */
+enum { TRI_BATCH_GRAPHS = 0, TRI_BATCH_SINGLE_LAUNCH = 1 };
+int tri_batch_set_mode(tri_batch* b, int32_t mode);
 int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile);
 
 /* ---- reference kernels (FP64, device pointers) -------------------------- */

@@ -36,13 +36,18 @@ def _solo(sc, precision):
         d.close()
 
 
+@pytest.mark.parametrize("single_launch", [False, True], ids=["graphs", "single_launch"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_batch_members_equal_solo_runs(precision):
+def test_batch_members_equal_solo_runs(precision, single_launch):
+    """Both launch modes: one launch per kernel type and step (CUDA graphs),
+    and one persistent launch per chunk of steps whose blocks take work items
+    with per-member dependencies."""
     scs = _members()
     solo = [_solo(sc, precision) for sc in scs]
     doms = [sc.to_domain(precision) for sc in scs]
     try:
         with Batch(doms) as b:
+            b.set_mode(single_launch)
             steps, updates = b.run()
         assert steps > 0 and updates > 0
         for sc, d, (fields, it, t) in zip(scs, doms, solo):

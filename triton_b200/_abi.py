@@ -16,6 +16,7 @@ TRI_OK, TRI_E_INVALID, TRI_E_CUDA, TRI_E_NOMEM, TRI_E_STATE, TRI_E_IO, TRI_E_TIM
 TRI_FP64, TRI_FP32 = 0, 1
 FIELD_H, FIELD_QX, FIELD_QY, FIELD_NMAN2, FIELD_DEM, FIELD_MAXH = range(6)
 EV_END, EV_PRINT, EV_OBS, EV_LOG = 1, 2, 4, 8
+BATCH_GRAPHS, BATCH_SINGLE_LAUNCH = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -95,6 +96,7 @@ _SIGS = {
     "tri_batch_wait": (C.c_int, [_vp, C.POINTER(BatchProgress)]),
     "tri_batch_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_batch_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "tri_batch_set_mode": (C.c_int, [_vp, C.c_int32]),
     "tri_selftest_division": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     "tri_kernel_compute_dt_and_sqrt_f64": (C.c_int, [C.c_int, C.c_double, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                                      C.c_double, _vp]),

@@ -68,6 +68,12 @@ class Batch:
     def set_shape(self, variant, rows_per_tile):
         check(lib().tri_batch_set_tuning(self._h, int(variant), int(rows_per_tile)))
 
+    def set_mode(self, single_launch):
+        """True: batched steps run in single persistent launches (members
+        advance without grid-wide barriers); False: one launch per kernel
+        type and step, captured as CUDA graphs (the default)."""
+        check(lib().tri_batch_set_mode(self._h, _abi.BATCH_SINGLE_LAUNCH if single_launch else _abi.BATCH_GRAPHS))
+
     def run(self, on_event=None, max_chunk=1 << 30):
         """Runs every member to its sim_duration.  After each batched advance,
         every member that raised an event gets ``on_event(member, events)``

@@ -41,6 +41,12 @@ struct tri_batch {
   std::vector<int32_t> bc_waves;
   int32_t* d_open = nullptr;  // members with open edges
   int n_open = 0, open_dim = 0;
+  // single-launch mode (TRI_BATCH_SINGLE_LAUNCH): progress counters per
+  // member, the members' forcing wave offsets, resident grid
+  int mode = TRI_BATCH_GRAPHS;
+  MemberProgress* d_prog = nullptr;
+  int32_t* d_woff = nullptr;
+  int steps_grid = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   double tuned_ms = 0;
@@ -95,6 +101,13 @@ MemberDev<T> member_dev(tri_domain* d, int rb, uint32_t& tiles, uint32_t& wet) {
   m.bc_nrows = a.bc_nrows;
   m.bc_v1 = (const T*)a.bc_v1;
   m.bc_v2 = (const T*)a.bc_v2;
+  m.wet_count = wet - m.wet_begin;
+  m.src_order = d->nsrc > 0 ? d->src_order : nullptr;
+  m.src_nw = d->nsrc > 0 ? (int)d->src_waves.size() - 1 : 0;
+  m.bc_order = d->nbc > 0 ? d->bc_order : nullptr;
+  m.bc_nw = d->nbc > 0 ? (int)d->bc_waves.size() - 1 : 0;
+  m.open = d->desc.open_boundaries ? 1 : 0;
+  m.src_woff = m.bc_woff = nullptr;  // set once the offsets are on the device
   return m;
 }
 
@@ -112,12 +125,32 @@ int build_table(tri_batch* b) {
   for (tri_domain* d : b->members) tab.push_back(member_dev<T>(d, b->rb, tiles, wet));
   b->ntiles = tiles;
   b->nwet = wet;
-  for (void** p : {&b->d_mem, (void**)&b->d_tile_mem, (void**)&b->d_wet_mem}) {
+  for (void** p : {&b->d_mem, (void**)&b->d_tile_mem, (void**)&b->d_wet_mem, (void**)&b->d_prog,
+                   (void**)&b->d_woff}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
   drop_graph(b);
   if (tab.empty()) return TRI_OK;
+  // single-launch mode: every member's wave offsets in one buffer, progress counters
+  std::vector<int32_t> woff;
+  std::vector<std::pair<size_t, size_t>> at(tab.size());
+  for (size_t m = 0; m < tab.size(); m++) {
+    const tri_domain* d = b->members[m];
+    at[m].first = woff.size();
+    if (tab[m].src_nw > 0) woff.insert(woff.end(), d->src_waves.begin(), d->src_waves.end());
+    at[m].second = woff.size();
+    if (tab[m].bc_nw > 0) woff.insert(woff.end(), d->bc_waves.begin(), d->bc_waves.end());
+  }
+  TRI_CUDA_TRY(cudaMalloc((void**)&b->d_woff, std::max<size_t>(woff.size(), 1) * sizeof(int32_t)));
+  if (!woff.empty())
+    TRI_CUDA_TRY(cudaMemcpy(b->d_woff, woff.data(), woff.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  for (size_t m = 0; m < tab.size(); m++) {
+    tab[m].src_woff = b->d_woff + at[m].first;
+    tab[m].bc_woff = b->d_woff + at[m].second;
+  }
+  TRI_CUDA_TRY(cudaMalloc((void**)&b->d_prog, tab.size() * sizeof(MemberProgress)));
+  b->steps_grid = batch_steps_grid<T>(b->variant);
   std::vector<int32_t> tm(tiles), wm(wet);
   for (size_t m = 0; m < tab.size(); m++) {
     std::fill(tm.begin() + tab[m].tile_begin, tm.begin() + tab[m].tile_end, (int32_t)m);
@@ -184,6 +217,8 @@ int build_items(tri_batch* b) {
     b->open_dim = std::max(b->open_dim, std::max(g.rows, g.cols));
   }
   if (b->d_open) cudaFree(b->d_open);
+  if (b->d_prog) cudaFree(b->d_prog);
+  if (b->d_woff) cudaFree(b->d_woff);
   b->d_open = nullptr;
   b->n_open = (int)open.size();
   if (!open.empty()) {
@@ -216,7 +251,27 @@ BatchArgs batch_args(tri_batch* b) {
   return a;
 }
 
+// Single-launch mode: n batched steps in launches of k_batch_steps, each
+// with fresh progress counters and ticket (tickets of one launch stay below
+// 2^31).
+int launch_batch_single(tri_batch* b, int n) {
+  const BatchArgs a = batch_args(b);
+  const uint64_t per_step = 2ull * (uint64_t)a.nm + (a.ntiles + 3) / 4 + a.nwet_blocks;
+  const int max_steps = (int)std::max<uint64_t>(1, std::min<uint64_t>(1u << 20, (1ull << 31) / per_step));
+  while (n > 0) {
+    const int k = std::min(n, max_steps);
+    TRI_CUDA_TRY(cudaMemsetAsync(b->d_prog, 0, b->members.size() * sizeof(MemberProgress), b->stream));
+    TRI_CUDA_TRY(cudaMemsetAsync(&b->d_ctl->ticket, 0, 2 * sizeof(uint32_t), b->stream));
+    const int rc = b->prec == TRI_FP64 ? launch_batch_steps<double>(a, b->d_prog, k, b->steps_grid, b->stream)
+                                       : launch_batch_steps<float>(a, b->d_prog, k, b->steps_grid, b->stream);
+    if (rc != TRI_OK) return rc;
+    n -= k;
+  }
+  return TRI_OK;
+}
+
 int launch_batch(tri_batch* b, int n) {
+  if (b->mode == TRI_BATCH_SINGLE_LAUNCH) return launch_batch_single(b, n);
   const BatchArgs a = batch_args(b);
   auto one = [&]() {
     return b->prec == TRI_FP64 ? launch_batch_step<double>(a, b->stream) : launch_batch_step<float>(a, b->stream);
@@ -286,7 +341,13 @@ int pull_members(tri_batch* b, tri_batch_progress* p) {
   memset(p, 0, sizeof(*p));
   for (tri_domain* d : b->members)
     TRI_CUDA_TRY(cudaMemcpyAsync(d->mirror, d->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, b->stream));
+  b->h_ctl->status = 0;
+  TRI_CUDA_TRY(cudaMemcpyAsync(&b->h_ctl->status, &b->d_ctl->status, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               b->stream));
   TRI_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (b->h_ctl->status != 0)
+    return set_error(TRI_E_TIMEOUT, "a dependency wait of the single-launch batch kernel gave up (status %d); the "
+                     "members' states are not valid", b->h_ctl->status);
   int64_t updates = 0;
   for (tri_domain* d : b->members) {
     const DevClock* m = d->mirror;
@@ -306,6 +367,8 @@ int pull_members(tri_batch* b, tri_batch_progress* p) {
 int reset_ctl(tri_batch* b) {
   b->h_ctl->halted = 0;
   b->h_ctl->tile_next = 0;
+  b->h_ctl->ticket = 0;
+  b->h_ctl->status = 0;
   TRI_CUDA_TRY(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
   return TRI_OK;
 }
@@ -379,6 +442,8 @@ int tri_batch_destroy(tri_batch* b) {
   if (b->d_src_items) cudaFree(b->d_src_items);
   if (b->d_bc_items) cudaFree(b->d_bc_items);
   if (b->d_open) cudaFree(b->d_open);
+  if (b->d_prog) cudaFree(b->d_prog);
+  if (b->d_woff) cudaFree(b->d_woff);
   for (int i = 0; i < 2; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -408,12 +473,13 @@ int tri_batch_advance(tri_batch* b, int32_t max_steps, tri_batch_progress* p) {
   if (rc != TRI_OK) return rc;
   if (runnable > 0 && max_steps > 0) {
     if ((rc = reset_ctl(b)) != TRI_OK) return rc;
-    // chunks of 8 batched steps, two in flight; stop once every runnable
-    // member has raised an event
+    // chunks of 8 batched steps (32 in single-launch mode), two in flight;
+    // stop once every runnable member has raised an event
+    const int chunk = b->mode == TRI_BATCH_SINGLE_LAUNCH ? 32 : 8;
     int left = max_steps, k = 0;
     bool done = false;
     while (left > 0 && !done) {
-      const int n = std::min(8, left);
+      const int n = std::min(chunk, left);
       rc = launch_batch(b, n);
       if (rc != TRI_OK) return rc;
       TRI_CUDA_TRY(cudaMemcpyAsync(&b->h_seen[k & 1], &b->d_ctl->halted, sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -449,6 +515,14 @@ int tri_batch_wait(tri_batch* b, tri_batch_progress* p) {
   TRI_CHECK_ARG(b && p, "null argument");
   b->launched = false;
   return pull_members(b, p);
+}
+
+int tri_batch_set_mode(tri_batch* b, int32_t mode) {
+  TRI_CHECK_ARG(b, "null batch");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
+  TRI_CHECK_ARG(mode == TRI_BATCH_GRAPHS || mode == TRI_BATCH_SINGLE_LAUNCH, "unknown batch mode %d", mode);
+  b->mode = mode;
+  return TRI_OK;
 }
 
 int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile) {

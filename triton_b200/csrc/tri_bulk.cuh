@@ -14,6 +14,10 @@ constexpr uint32_t kSpinLimit = 1u << 24;
 // Device-side status codes (DevClock::status).
 constexpr int32_t kStatusStageTimeout = 1;
 constexpr int32_t kStatusTestWait = 2;  // the wait of the test hook gave up (tri_domain_set_wait_test)
+constexpr int32_t kStatusStepWait = 3;  // a wait of the single-launch batch kernel gave up (k_batch_steps)
+// Polls of one dependency wait of k_batch_steps (with 128 ns sleeps: about
+// 2 s, where the dependencies it waits for take micro- to milliseconds).
+constexpr uint32_t kStepWaitPolls = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -62,6 +66,26 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
       "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
       "r"(bytes)
       : "memory");
+}
+
+// Invalidates an mbarrier whose phases are all complete, so its shared
+// memory can hold a new one (a block that stages several tiles in turn).
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Orders this thread's view of global memory (writes other blocks made
+// visible to it by an acquire) before its later bulk copies, which read
+// through the async proxy.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// Acquire load of a counter other blocks increment (gpu scope).
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
 // Copies 'bytes' (a multiple of 16) from global 'src' (16-byte aligned) to

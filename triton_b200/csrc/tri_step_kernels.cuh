@@ -1238,16 +1238,10 @@ __global__ void k_batch_open_bc(const MemberDev<T>* __restrict__ mem, const int3
   open_bc_item<T>(M.clk, M.sb, M.rows, M.cols, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// Sparse forcing of a batch: items are (member, index) pairs of one
-// conflict-free wave (a member's own waves keep its index order).
+// Point source `id` of member M (compute_flow, kernels.h:51-84).
 template <typename T>
-__global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2* __restrict__ items, int count) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= count) return;
-  const int m = items[k].x, id = items[k].y;
-  const MemberDev<T>& M = mem[m];
+__device__ __forceinline__ void source_apply(const MemberDev<T>& M, int id) {
   DevClock* clk = M.clk;
-  if (!clk->active) return;
   const int lo = clk->src_idx_low, hi = clk->src_idx_high;
   const T dt = T(clk->global_dt), simtime = T(clk->t_step);
   T* h = M.sb.H(clk->dst);
@@ -1268,6 +1262,17 @@ __global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2
   atomicAdd(&clk->acc_step[kAccSources], (double)hs);
 }
 
+// Sparse forcing of a batch: items are (member, index) pairs of one
+// conflict-free wave (a member's own waves keep its index order).
+template <typename T>
+__global__ void k_batch_sources(const MemberDev<T>* __restrict__ mem, const int2* __restrict__ items, int count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const MemberDev<T>& M = mem[items[k].x];
+  if (!M.clk->active) return;
+  source_apply<T>(M, items[k].y);
+}
+
 template <typename T>
 __global__ void k_batch_extbc(const MemberDev<T>* __restrict__ mem, const int2* __restrict__ items, int count) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1276,6 +1281,194 @@ __global__ void k_batch_extbc(const MemberDev<T>* __restrict__ mem, const int2* 
   if (!M.clk->active) return;
   extbc_apply<T>(M.clk, M.sb, M.bed, M.n2, items[k].y, M.bc_cells, M.bc_types, M.bc_start, M.bc_nrows, M.bc_v1,
                  M.bc_v2, M.rows, M.cols);
+}
+
+// ===========================================================================
+// Single-launch batches: k_batch_steps advances every member of a batch by
+// `nsteps` of its own time steps in ONE launch.  Blocks stay resident and take
+// work items from a ticket counter in a fixed order; per batched step s:
+//   nm clock items (one per member), then the flux tiles of all members in
+//   groups of four (one per warp), then nm forcing items (a member's point
+//   sources, open-edge ghosts and external-boundary cells, wave by wave), then
+//   the wet-dry/dt blocks of all members.
+// An item waits only for items of its own member with lower tickets (flux
+// tiles for the member's clock of step s, forcing for all its flux tiles of
+// step s, wet-dry blocks for its forcing of step s, the clock of step s+1 for
+// all its wet-dry blocks of step s), counted in MemberProgress.  Lower
+// tickets were taken by blocks that are running, so the lowest unfinished
+// ticket can always proceed and every wait ends: members advance without a
+// barrier across members or across the grid, and the tail of one phase
+// overlaps the next phase of members that are ahead.  Waits are bounded
+// (kStepWaitPolls); one that gives up records a status, and the others then
+// give up at once.  Producers publish with a gpu-scope fence from every
+// thread, a block (or warp) barrier and a fenced increment by one thread;
+// consumers poll with an acquire load, then every thread acquires after a
+// barrier (and issues a proxy fence before bulk copies).
+// ===========================================================================
+template <typename T>
+__device__ __forceinline__ void forcing_block(const MemberDev<T>& M) {
+  DevClock* clk = M.clk;
+  for (int w = 0; w < M.src_nw; ++w) {
+    for (int i = M.src_woff[w] + (int)threadIdx.x; i < M.src_woff[w + 1]; i += blockDim.x)
+      source_apply<T>(M, M.src_order[i]);
+    __syncthreads();
+  }
+  if (M.open) {
+    const int n = max(M.rows, M.cols);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) open_bc_item<T>(clk, M.sb, M.rows, M.cols, k);
+    __syncthreads();
+  }
+  for (int w = 0; w < M.bc_nw; ++w) {
+    for (int i = M.bc_woff[w] + (int)threadIdx.x; i < M.bc_woff[w + 1]; i += blockDim.x)
+      extbc_apply<T>(clk, M.sb, M.bed, M.n2, M.bc_order[i], M.bc_cells, M.bc_types, M.bc_start, M.bc_nrows,
+                     M.bc_v1, M.bc_v2, M.rows, M.cols);
+    __syncthreads();
+  }
+}
+
+// Bounded wait until *counter >= target (acquire).  A wait that gives up
+// records the status; once any wait of the launch has given up, the others
+// give up at once instead of waiting out their own limit.
+__device__ __forceinline__ void steps_wait(const uint32_t* counter, uint32_t target, BatchCtl* ctl) {
+  for (uint32_t it = 0; it < kStepWaitPolls; ++it) {
+    if (ld_acquire_u32(counter) >= target) return;
+    if (*reinterpret_cast<volatile int32_t*>(&ctl->status) != 0) return;
+    if (it > 32) __nanosleep(128);
+  }
+  atomicExch(&ctl->status, kStatusStepWait);
+}
+
+// Every thread's writes are made visible at gpu scope, then one count
+// (thread 0 fences again after the barrier, so the count is released after
+// every thread's writes).
+__device__ __forceinline__ void publish_block(uint32_t* counter) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+  }
+}
+
+// Thread 0 waits for *counter >= target, then, after a block barrier, every
+// thread acquires the counter itself, so each thread's later reads see what
+// the producers published.
+__device__ __forceinline__ void acquire_block(const uint32_t* counter, uint32_t target, BatchCtl* ctl) {
+  if (threadIdx.x == 0) steps_wait(counter, target, ctl);
+  __syncthreads();
+  (void)ld_acquire_u32(counter);
+}
+
+// The kinds of block item.  The clock, forcing and wet-dry items are compiled
+// out of line, so their registers are allocated apart from the flux tile's
+// (the persistent loop keeps only a few values live across the calls).
+template <typename T>
+__device__ __forceinline__ void steps_flux_item(const MemberDev<T>* __restrict__ mem,
+                                                const int32_t* __restrict__ tile_member, uint32_t ntiles,
+                                                uint32_t r, uint32_t s, BatchCtl* __restrict__ ctl,
+                                                MemberProgress* __restrict__ prog) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t tile = 4u * r + (uint32_t)warp;  // one tile per warp
+  if (tile >= ntiles) return;
+  const int m = tile_member[tile];
+  const MemberDev<T>& M = mem[m];
+  if (lane == 0) steps_wait(&prog[m].clock, s + 1, ctl);
+  __syncwarp();
+  (void)ld_acquire_u32(&prog[m].clock);  // every lane acquires what the clock item published
+  if (M.clk->active) {
+    const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
+                                     M.hextra);
+    flux_tile<T, false>(X, tile - M.tile_begin, lane);
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence();
+    atomicAdd(&prog[m].flux, 1u);
+  }
+}
+
+template <typename T>
+__device__ __noinline__ void steps_clock_item(const MemberDev<T>& M, uint32_t m, uint32_t s,
+                                              BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog) {
+  steps_wait(&prog[m].wet, s * M.wet_count, ctl);
+  if (clock_step(M.clk)) atomicAdd(&ctl->halted, 1);
+  __threadfence();
+  atomicAdd(&prog[m].clock, 1u);
+}
+
+template <typename T>
+__device__ __noinline__ void steps_forcing_item(const MemberDev<T>& M, uint32_t m, uint32_t s,
+                                                BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog) {
+  acquire_block(&prog[m].flux, (s + 1) * (M.tile_end - M.tile_begin), ctl);
+  if (M.clk->active) forcing_block<T>(M);
+  publish_block(&prog[m].forcing);
+}
+
+// Returns true when the block must take no further item (a copy group of
+// its staging never completed, so its shared memory may still be written).
+template <typename T>
+__device__ __noinline__ bool steps_wet_item(const MemberDev<T>* __restrict__ mem,
+                                            const int32_t* __restrict__ wet_member, uint32_t r, uint32_t s,
+                                            BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog,
+                                            unsigned char* smem) {
+  using S = WetStage<T>;
+  const int m = wet_member[r];
+  const MemberDev<T>& M = mem[m];
+  acquire_block(&prog[m].forcing, s + 1, ctl);
+  DevClock* clk = M.clk;
+  bool broken = false;
+  if (clk->active) {
+    fence_proxy_async_global();  // the bulk copies read what other blocks wrote
+    const uint32_t local = r - M.wet_begin;
+    if (local == 0 && threadIdx.x == 0) fold_accounts(clk);
+    const unsigned long long key =
+        wetdry_staged<T>(clk, M.sb, M.bed, M.maxh, M.rows, M.cols, M.hextra, M.arrival, M.arrival_depth,
+                         (int)(local % M.wet_nbx), (int)(local / M.wet_nbx), reinterpret_cast<T*>(smem));
+    block_min_into(key, &clk->dt_key[clk->wr]);
+    broken = __syncthreads_or(clk->status == kStatusStageTimeout) != 0;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kData);
+    if (!broken && threadIdx.x < S::kGroups) mbar_inval(&bar[threadIdx.x]);
+  }
+  publish_block(&prog[m].wet);
+  return broken;
+}
+
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    k_batch_steps(const MemberDev<T>* __restrict__ mem, int nm, const int32_t* __restrict__ tile_member,
+                  uint32_t ntiles, const int32_t* __restrict__ wet_member, uint32_t nwet, int nsteps,
+                  BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog) {
+  extern __shared__ __align__(128) unsigned char wet_smem[];
+  __shared__ uint32_t s_ticket;
+  const uint32_t nflux = (ntiles + 3) / 4;
+  const uint32_t per_step = 2u * (uint32_t)nm + nflux + nwet;
+  const uint32_t total = per_step * (uint32_t)nsteps;
+  while (true) {
+    __syncthreads();  // the previous item is finished by every thread
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl->ticket, 1u);
+    __syncthreads();
+    const uint32_t t = s_ticket;
+    if (t >= total) return;
+    const uint32_t s = t / per_step;
+    uint32_t r = t - s * per_step;
+    if (r < (uint32_t)nm) {  // clock of member r, step s
+      if (threadIdx.x == 0) steps_clock_item<T>(mem[r], r, s, ctl, prog);
+      continue;
+    }
+    r -= (uint32_t)nm;
+    if (r < nflux) {
+      steps_flux_item<T>(mem, tile_member, ntiles, r, s, ctl, prog);
+      continue;
+    }
+    r -= nflux;
+    if (r < (uint32_t)nm) {
+      steps_forcing_item<T>(mem[r], r, s, ctl, prog);
+      continue;
+    }
+    r -= (uint32_t)nm;
+    if (steps_wet_item<T>(mem, wet_member, r, s, ctl, prog, wet_smem)) return;
+  }
 }
 
 }  // namespace tri

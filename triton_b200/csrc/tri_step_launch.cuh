@@ -149,8 +149,34 @@ int launch_batch_step(const BatchArgs& a, cudaStream_t s) {
   return TRI_OK;
 }
 
+// Single-launch kernel of a register-budget variant (the first two budgets).
+template <typename T>
+auto steps_kernel(int variant) -> decltype(&k_batch_steps<T, FluxBudget<T>::v0>) {
+  return variant == 0 ? &k_batch_steps<T, FluxBudget<T>::v0> : &k_batch_steps<T, FluxBudget<T>::v1>;
+}
+
+template <typename T>
+int batch_steps_grid(int variant) {
+  int sms = 148, dev = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel<T>(variant), 128, WetStage<T>::kBytes);
+  return sms * std::max(per_sm, 1);
+}
+
+template <typename T>
+int launch_batch_steps(const BatchArgs& a, MemberProgress* prog, int nsteps, int grid, cudaStream_t s) {
+  const MemberDev<T>* mem = (const MemberDev<T>*)a.mem;
+  steps_kernel<T>(a.flux_variant)<<<grid, 128, WetStage<T>::kBytes, s>>>(
+      mem, a.nm, a.tile_member, a.ntiles, a.wet_member, a.nwet_blocks, nsteps, a.ctl, prog);
+  TRI_CUDA_TRY(cudaGetLastError());
+  return TRI_OK;
+}
+
 template <typename T>
 int prepare_kernels() {
+  for (int v = 0; v < 2; v++)
+    TRI_CUDA_TRY(cudaFuncSetAttribute(steps_kernel<T>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)WetStage<T>::kBytes));
   TRI_CUDA_TRY(cudaFuncSetAttribute(k_wetdry_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)WetStage<T>::kBytes));
   TRI_CUDA_TRY(cudaFuncSetAttribute(k_batch_wetdry<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -110,6 +110,14 @@ struct BatchArgs {
 };
 template <typename T>
 int launch_batch_step(const BatchArgs& a, cudaStream_t s);
+// Single-launch mode: nsteps batched steps in one launch of k_batch_steps
+// (the control block's ticket and status and the progress counters must be
+// zero); grid: the blocks resident at once (batch_steps_grid).  Register
+// budget: variant 0 or (any other) 1 of FluxBudget.
+template <typename T>
+int launch_batch_steps(const BatchArgs& a, MemberProgress* prog, int nsteps, int grid, cudaStream_t s);
+template <typename T>
+int batch_steps_grid(int variant);
 template <typename T>
 void batch_flux_occupancy(int variant, int* per_sm);
 
@@ -128,6 +136,10 @@ extern template void flux_occupancy<double>(int, int*);
 extern template void flux_occupancy<float>(int, int*);
 extern template int launch_batch_step<double>(const BatchArgs&, cudaStream_t);
 extern template int launch_batch_step<float>(const BatchArgs&, cudaStream_t);
+extern template int launch_batch_steps<double>(const BatchArgs&, MemberProgress*, int, int, cudaStream_t);
+extern template int launch_batch_steps<float>(const BatchArgs&, MemberProgress*, int, int, cudaStream_t);
+extern template int batch_steps_grid<double>(int);
+extern template int batch_steps_grid<float>(int);
 extern template void batch_flux_occupancy<double>(int, int*);
 extern template void batch_flux_occupancy<float>(int, int*);
 

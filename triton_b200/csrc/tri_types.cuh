@@ -125,11 +125,26 @@ struct MemberDev {
   const T* hyg_v;
   const int32_t *bc_cells, *bc_types, *bc_start, *bc_nrows;
   const T *bc_v1, *bc_v2;
+  // single-launch mode (k_batch_steps): the member's wet-dry block count and
+  // its forcing as conflict-free waves of its own items (order: device item
+  // indices wave after wave, woff: nw+1 wave offsets), open edges
+  uint32_t wet_count;
+  const int32_t *src_order, *src_woff, *bc_order, *bc_woff;
+  int src_nw, bc_nw, open;
 };
 
 struct BatchCtl {
   uint32_t tile_next;  // flux tile queue, reset every batched step
   int32_t halted;      // members that raised an event during this advance call
+  uint32_t ticket;     // single-launch mode: next work item, reset by every launch
+  int32_t status;      // single-launch mode: nonzero if a bounded wait gave up
+};
+
+// Single-launch mode: per member, cumulative counts of finished work items
+// within one launch (zeroed before it): clock steps, flux tiles, forcing
+// passes, wet-dry blocks.
+struct MemberProgress {
+  uint32_t clock, flux, forcing, wet;
 };
 
 }  // namespace tri
