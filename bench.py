@@ -91,6 +91,23 @@ def _issue_bound(precision):
             "source": f"profiles/{fname} (ncu, one launch in the timed steps)"}
 
 
+def _fp64_pipe(precision, launch_s, sm_mhz):
+    """The flux kernel against the FP64 pipe: its FP64 warp instructions per
+    launch (committed ncu summary of the same workload and launch shape) over
+    the launch time measured here, against the pipe's peak of 148 SMs x 4
+    schedulers x 1/2 warp instruction per cycle (16 FP64 lanes per scheduler)
+    at the SM clock sampled during the run."""
+    fname = f"k_flux_update_thacker2048_{precision}.txt"
+    n = _profile_metric(fname, "smsp__inst_executed_pipe_fp64.sum")
+    if n is None or not launch_s or not sm_mhz:
+        return None
+    achieved = n / launch_s / 1e9
+    peak = 148 * 4 * 0.5 * sm_mhz * 1e6 / 1e9
+    return {"bound": "fp64_pipe", "unit": "G warp-instructions/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "fp64_warp_instructions_per_launch": n,
+            "source": f"profiles/{fname} (instruction count), launch time and SM clock of this run"}
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -393,6 +410,12 @@ def form_ensemble(args, stream):
             ens[f"{prec}_batched"] = p.cell_updates / (ms / 1000.0)
             ens[f"{prec}_batched_ms_per_step"] = ms / args.ens_steps
             ens[f"{prec}_batched_shape"] = {k: tune[k] for k in ("variant", "rows_per_tile")}
+            # the same steps in single persistent launches (per-member
+            # dependencies instead of a launch per kernel type and step)
+            b.set_mode(True)
+            b.advance(args.warmup)
+            p, ms = _timed(stream, lambda: b.advance(args.ens_steps))
+            ens[f"{prec}_batched_single_launch"] = p.cell_updates / (ms / 1000.0)
             b.close()
         def solo():  # the same members as plain FP64 runs, one after another
             u = 0
@@ -667,6 +690,7 @@ def main():
                          "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
                          "wetdry_dt_avg_launch_ms": wet_ms / max(wet_n, 1),
                          "issue_bound": _issue_bound(args.precision),
+                         "fp64_pipe": _fp64_pipe(args.precision, flux_avg_s, (clocks or {}).get("sm_mhz")),
                          "launch_timing": f"CUDA event pair around each of {flux_n} flux launches, in a "
                                           f"second pass of the same {args.steps} steps right after the "
                                           f"timed region"},
