@@ -9,7 +9,11 @@
 // without idle SMs), the sparse forcing in conflict-free waves of (member,
 // item) pairs, and one wet-dry/dt kernel over all members' bands, each member
 // folding its own dt minimum.  Steps are launched as CUDA graphs of 8 batched
-// steps; the host checks after each graph how many members have halted.
+// steps; the host checks after each graph how many members have halted.  In
+// single-launch mode (tri_batch_set_mode) one persistent launch of
+// k_batch_steps runs a chunk of 32 batched steps instead: its blocks take the
+// same work items from a ticket counter and wait, bounded, only for their own
+// member's earlier items.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -217,8 +221,6 @@ int build_items(tri_batch* b) {
     b->open_dim = std::max(b->open_dim, std::max(g.rows, g.cols));
   }
   if (b->d_open) cudaFree(b->d_open);
-  if (b->d_prog) cudaFree(b->d_prog);
-  if (b->d_woff) cudaFree(b->d_woff);
   b->d_open = nullptr;
   b->n_open = (int)open.size();
   if (!open.empty()) {
@@ -253,15 +255,17 @@ BatchArgs batch_args(tri_batch* b) {
 
 // Single-launch mode: n batched steps in launches of k_batch_steps, each
 // with fresh progress counters and ticket (tickets of one launch stay below
-// 2^31).
+// 2^31); the status word is cleared once, so a timeout in any launch of the
+// chunk reaches the host.
 int launch_batch_single(tri_batch* b, int n) {
   const BatchArgs a = batch_args(b);
   const uint64_t per_step = 2ull * (uint64_t)a.nm + (a.ntiles + 3) / 4 + a.nwet_blocks;
   const int max_steps = (int)std::max<uint64_t>(1, std::min<uint64_t>(1u << 20, (1ull << 31) / per_step));
+  TRI_CUDA_TRY(cudaMemsetAsync(&b->d_ctl->status, 0, sizeof(int32_t), b->stream));
   while (n > 0) {
     const int k = std::min(n, max_steps);
     TRI_CUDA_TRY(cudaMemsetAsync(b->d_prog, 0, b->members.size() * sizeof(MemberProgress), b->stream));
-    TRI_CUDA_TRY(cudaMemsetAsync(&b->d_ctl->ticket, 0, 2 * sizeof(uint32_t), b->stream));
+    TRI_CUDA_TRY(cudaMemsetAsync(&b->d_ctl->ticket, 0, sizeof(uint32_t), b->stream));
     const int rc = b->prec == TRI_FP64 ? launch_batch_steps<double>(a, b->d_prog, k, b->steps_grid, b->stream)
                                        : launch_batch_steps<float>(a, b->d_prog, k, b->steps_grid, b->stream);
     if (rc != TRI_OK) return rc;
