@@ -274,6 +274,13 @@ int tri_batch_autotune(tri_batch* b, int32_t trial_steps, tri_tuning* out);
  * return TRI_E_TIMEOUT. */
 enum { TRI_BATCH_GRAPHS = 0, TRI_BATCH_SINGLE_LAUNCH = 1 };
 int tri_batch_set_mode(tri_batch* b, int32_t mode);
+/* Test hook of the single-launch mode (no reference counterpart): with
+ * polls > 0 the first clock item of the next advances also waits for a count
+ * that no item ever reaches, giving up after `polls` polls, so the advance
+ * returns TRI_E_TIMEOUT with nothing else wrong (every other wait then gives
+ * up at once; the members' states are not valid afterwards).  0 turns it
+ * off.  No effect in TRI_BATCH_GRAPHS mode. */
+int tri_batch_set_wait_test(tri_batch* b, uint32_t polls);
 int tri_batch_set_tuning(tri_batch* b, int32_t variant, int32_t rows_per_tile);
 
 /* ---- reference kernels (FP64, device pointers) -------------------------- */

@@ -46,3 +46,46 @@ def test_wait_that_runs_out_returns_timeout_and_context_stays_usable():
     finally:
         ref.close()
         hooked.close()
+
+
+def test_single_launch_batch_wait_that_runs_out_returns_timeout():
+    """The persistent batch kernel's dependency waits are bounded too: with
+    the batch's test hook the first clock item waits for a count no item ever
+    reaches; it gives up, every other wait then gives up at once, the launch
+    ends and the advance returns TRI_E_TIMEOUT.  The context stays usable: a
+    new batch over fresh members steps normally afterwards."""
+    from triton_b200.batch import Batch
+
+    scs = []
+    for i in range(3):
+        sc = scenarios.dambreak(n=64 + 16 * i, dx=1.0, radius=12.0, depth=4.0, duration=10.0)
+        sc.print_interval = 10.0
+        scs.append(sc)
+    doms = [sc.to_domain() for sc in scs]
+    try:
+        with Batch(doms) as b:
+            b.set_mode(True)
+            b.set_wait_test(1000)
+            with pytest.raises(_abi.TriError) as e:
+                b.advance(8)
+            assert e.value.code == _abi.TRI_E_TIMEOUT
+            assert "single-launch" in str(e.value)
+    finally:
+        for d in doms:
+            d.close()
+    fresh = [sc.to_domain() for sc in scs]
+    solo = [sc.to_domain() for sc in scs]
+    try:
+        with Batch(fresh) as b:
+            b.set_mode(True)
+            p = b.advance(8)
+            assert p.steps == 8
+        for d in solo:
+            steps, _ = d.advance(8)
+            assert steps == 8
+        for f, s in zip(fresh, solo):
+            for a, c in zip(_fields(f), _fields(s)):
+                assert np.array_equal(a, c)
+    finally:
+        for d in fresh + solo:
+            d.close()

@@ -97,6 +97,7 @@ _SIGS = {
     "tri_batch_autotune": (C.c_int, [_vp, C.c_int32, C.POINTER(Tuning)]),
     "tri_batch_set_tuning": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "tri_batch_set_mode": (C.c_int, [_vp, C.c_int32]),
+    "tri_batch_set_wait_test": (C.c_int, [_vp, C.c_uint32]),
     "tri_selftest_division": (C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     "tri_kernel_compute_dt_and_sqrt_f64": (C.c_int, [C.c_int, C.c_double, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                                      C.c_double, _vp]),

@@ -74,6 +74,12 @@ class Batch:
         type and step, captured as CUDA graphs (the default)."""
         check(lib().tri_batch_set_mode(self._h, _abi.BATCH_SINGLE_LAUNCH if single_launch else _abi.BATCH_GRAPHS))
 
+    def set_wait_test(self, polls):
+        """Single-launch mode test hook: the next advances' first clock item
+        waits for a count that is never reached and gives up after `polls`
+        polls (TRI_E_TIMEOUT); 0 turns it off."""
+        check(lib().tri_batch_set_wait_test(self._h, int(polls)))
+
     def run(self, on_event=None, max_chunk=1 << 30):
         """Runs every member to its sim_duration.  After each batched advance,
         every member that raised an event gets ``on_event(member, events)``

@@ -51,6 +51,7 @@ struct tri_batch {
   MemberProgress* d_prog = nullptr;
   int32_t* d_woff = nullptr;
   int steps_grid = 0;
+  uint32_t wait_test = 0;  // tri_batch_set_wait_test
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   double tuned_ms = 0;
@@ -373,6 +374,7 @@ int reset_ctl(tri_batch* b) {
   b->h_ctl->tile_next = 0;
   b->h_ctl->ticket = 0;
   b->h_ctl->status = 0;
+  b->h_ctl->wait_test = b->wait_test;
   TRI_CUDA_TRY(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
   return TRI_OK;
 }
@@ -526,6 +528,13 @@ int tri_batch_set_mode(tri_batch* b, int32_t mode) {
   if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
   TRI_CHECK_ARG(mode == TRI_BATCH_GRAPHS || mode == TRI_BATCH_SINGLE_LAUNCH, "unknown batch mode %d", mode);
   b->mode = mode;
+  return TRI_OK;
+}
+
+int tri_batch_set_wait_test(tri_batch* b, uint32_t polls) {
+  TRI_CHECK_ARG(b, "null batch");
+  if (b->launched) return set_error(TRI_E_STATE, "batch has launched steps; call tri_batch_wait first");
+  b->wait_test = polls;
   return TRI_OK;
 }
 

@@ -1300,10 +1300,12 @@ __global__ void k_batch_extbc(const MemberDev<T>* __restrict__ mem, const int2* 
 // barrier across members or across the grid, and the tail of one phase
 // overlaps the next phase of members that are ahead.  Waits are bounded
 // (kStepWaitPolls); one that gives up records a status, and the others then
-// give up at once.  Producers publish with a gpu-scope fence from every
-// thread, a block (or warp) barrier and a fenced increment by one thread;
-// consumers poll with an acquire load, then every thread acquires after a
-// barrier (and issues a proxy fence before bulk copies).
+// give up at once.  A producer publishes as a grid barrier does: a block (or
+// warp) barrier, then one thread's gpu-scope fence and increment; a consumer
+// polls with one thread's acquire load, then a block (or warp) barrier (and
+// a proxy fence before bulk copies).  A block takes its next ticket while
+// its current item runs, and acquires a (member, step) dependency once for
+// consecutive items of the same kind.
 // ===========================================================================
 template <typename T>
 __device__ __forceinline__ void forcing_block(const MemberDev<T>& M) {
@@ -1329,8 +1331,9 @@ __device__ __forceinline__ void forcing_block(const MemberDev<T>& M) {
 // Bounded wait until *counter >= target (acquire).  A wait that gives up
 // records the status; once any wait of the launch has given up, the others
 // give up at once instead of waiting out their own limit.
-__device__ __forceinline__ void steps_wait(const uint32_t* counter, uint32_t target, BatchCtl* ctl) {
-  for (uint32_t it = 0; it < kStepWaitPolls; ++it) {
+__device__ __forceinline__ void steps_wait(const uint32_t* counter, uint32_t target, BatchCtl* ctl,
+                                           uint32_t polls = kStepWaitPolls) {
+  for (uint32_t it = 0; it < polls; ++it) {
     if (ld_acquire_u32(counter) >= target) return;
     if (*reinterpret_cast<volatile int32_t*>(&ctl->status) != 0) return;
     if (it > 32) __nanosleep(128);
@@ -1338,11 +1341,10 @@ __device__ __forceinline__ void steps_wait(const uint32_t* counter, uint32_t tar
   atomicExch(&ctl->status, kStatusStepWait);
 }
 
-// Every thread's writes are made visible at gpu scope, then one count
-// (thread 0 fences again after the barrier, so the count is released after
-// every thread's writes).
+// Publishes a block's item: after a block barrier (every thread's writes of
+// the item happen before it), one thread makes them visible at gpu scope
+// (a cumulative fence) and counts the item; the pattern of a grid barrier.
 __device__ __forceinline__ void publish_block(uint32_t* counter) {
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -1350,37 +1352,40 @@ __device__ __forceinline__ void publish_block(uint32_t* counter) {
   }
 }
 
-// Thread 0 waits for *counter >= target, then, after a block barrier, every
-// thread acquires the counter itself, so each thread's later reads see what
-// the producers published.
+// Thread 0 waits for *counter >= target (acquire); the block barrier after
+// it orders every thread's later reads after what the producers published.
 __device__ __forceinline__ void acquire_block(const uint32_t* counter, uint32_t target, BatchCtl* ctl) {
   if (threadIdx.x == 0) steps_wait(counter, target, ctl);
   __syncthreads();
-  (void)ld_acquire_u32(counter);
 }
 
 // The kinds of block item.  The clock, forcing and wet-dry items are compiled
 // out of line, so their registers are allocated apart from the flux tile's
 // (the persistent loop keeps only a few values live across the calls).
+// *seen caches the last (member, step) whose clock this warp has acquired:
+// consecutive tiles of one member and step wait once.
 template <typename T>
 __device__ __forceinline__ void steps_flux_item(const MemberDev<T>* __restrict__ mem,
                                                 const int32_t* __restrict__ tile_member, uint32_t ntiles,
                                                 uint32_t r, uint32_t s, BatchCtl* __restrict__ ctl,
-                                                MemberProgress* __restrict__ prog) {
+                                                MemberProgress* __restrict__ prog, uint32_t* seen_m,
+                                                uint32_t* seen_s) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t tile = 4u * r + (uint32_t)warp;  // one tile per warp
   if (tile >= ntiles) return;
   const int m = tile_member[tile];
   const MemberDev<T>& M = mem[m];
-  if (lane == 0) steps_wait(&prog[m].clock, s + 1, ctl);
-  __syncwarp();
-  (void)ld_acquire_u32(&prog[m].clock);  // every lane acquires what the clock item published
+  if (*seen_m != (uint32_t)m || *seen_s != s) {
+    if (lane == 0) steps_wait(&prog[m].clock, s + 1, ctl);
+    __syncwarp();
+    *seen_m = (uint32_t)m;
+    *seen_s = s;
+  }
   if (M.clk->active) {
     const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
                                      M.hextra);
     flux_tile<T, false>(X, tile - M.tile_begin, lane);
   }
-  __threadfence();
   __syncwarp();
   if (lane == 0) {
     __threadfence();
@@ -1391,6 +1396,10 @@ __device__ __forceinline__ void steps_flux_item(const MemberDev<T>* __restrict__
 template <typename T>
 __device__ __noinline__ void steps_clock_item(const MemberDev<T>& M, uint32_t m, uint32_t s,
                                               BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog) {
+  // test hook (tri_batch_set_wait_test): the first clock item waits for a
+  // count no item ever reaches, bounded by ctl->wait_test polls, so the
+  // handling of a wait that gave up can be tested with nothing else wrong
+  if (ctl->wait_test != 0 && m == 0 && s == 0) steps_wait(&prog[0].clock, 0xFFFFFFFFu, ctl, ctl->wait_test);
   steps_wait(&prog[m].wet, s * M.wet_count, ctl);
   if (clock_step(M.clk)) atomicAdd(&ctl->halted, 1);
   __threadfence();
@@ -1407,15 +1416,21 @@ __device__ __noinline__ void steps_forcing_item(const MemberDev<T>& M, uint32_t 
 
 // Returns true when the block must take no further item (a copy group of
 // its staging never completed, so its shared memory may still be written).
+// The forcing of (member, step) is acquired once per block: consecutive
+// bands of one member and step do not wait again.
 template <typename T>
 __device__ __noinline__ bool steps_wet_item(const MemberDev<T>* __restrict__ mem,
                                             const int32_t* __restrict__ wet_member, uint32_t r, uint32_t s,
                                             BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog,
-                                            unsigned char* smem) {
+                                            unsigned char* smem, uint32_t* seen_m, uint32_t* seen_s) {
   using S = WetStage<T>;
   const int m = wet_member[r];
   const MemberDev<T>& M = mem[m];
-  acquire_block(&prog[m].forcing, s + 1, ctl);
+  if (*seen_m != (uint32_t)m || *seen_s != s) {
+    acquire_block(&prog[m].forcing, s + 1, ctl);
+    *seen_m = (uint32_t)m;
+    *seen_s = s;
+  }
   DevClock* clk = M.clk;
   bool broken = false;
   if (clk->active) {
@@ -1434,40 +1449,40 @@ __device__ __noinline__ bool steps_wet_item(const MemberDev<T>* __restrict__ mem
   return broken;
 }
 
+// The next ticket is taken while the current item runs (its atomic's latency
+// hidden); a block then holds two tickets, but its next one is higher than
+// its current one, so the lowest unfinished ticket is always a current item
+// and can proceed.
 template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB)
     k_batch_steps(const MemberDev<T>* __restrict__ mem, int nm, const int32_t* __restrict__ tile_member,
                   uint32_t ntiles, const int32_t* __restrict__ wet_member, uint32_t nwet, int nsteps,
                   BatchCtl* __restrict__ ctl, MemberProgress* __restrict__ prog) {
   extern __shared__ __align__(128) unsigned char wet_smem[];
-  __shared__ uint32_t s_ticket;
+  __shared__ uint32_t s_ticket[2];
   const uint32_t nflux = (ntiles + 3) / 4;
   const uint32_t per_step = 2u * (uint32_t)nm + nflux + nwet;
   const uint32_t total = per_step * (uint32_t)nsteps;
-  while (true) {
-    __syncthreads();  // the previous item is finished by every thread
-    if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl->ticket, 1u);
-    __syncthreads();
-    const uint32_t t = s_ticket;
+  if (threadIdx.x == 0) s_ticket[0] = atomicAdd(&ctl->ticket, 1u);
+  __syncthreads();
+  uint32_t fm = 0xFFFFFFFFu, fs = 0, wm = 0xFFFFFFFFu, ws = 0;  // last acquired (member, step) per kind
+  for (int cur = 0;; cur ^= 1) {
+    const uint32_t t = s_ticket[cur];
     if (t >= total) return;
+    if (threadIdx.x == 0) s_ticket[cur ^ 1] = atomicAdd(&ctl->ticket, 1u);
     const uint32_t s = t / per_step;
     uint32_t r = t - s * per_step;
     if (r < (uint32_t)nm) {  // clock of member r, step s
       if (threadIdx.x == 0) steps_clock_item<T>(mem[r], r, s, ctl, prog);
-      continue;
-    }
-    r -= (uint32_t)nm;
-    if (r < nflux) {
-      steps_flux_item<T>(mem, tile_member, ntiles, r, s, ctl, prog);
-      continue;
-    }
-    r -= nflux;
-    if (r < (uint32_t)nm) {
+    } else if ((r -= (uint32_t)nm) < nflux) {
+      steps_flux_item<T>(mem, tile_member, ntiles, r, s, ctl, prog, &fm, &fs);
+    } else if ((r -= nflux) < (uint32_t)nm) {
       steps_forcing_item<T>(mem[r], r, s, ctl, prog);
-      continue;
+    } else {
+      r -= (uint32_t)nm;
+      if (steps_wet_item<T>(mem, wet_member, r, s, ctl, prog, wet_smem, &wm, &ws)) return;
     }
-    r -= (uint32_t)nm;
-    if (steps_wet_item<T>(mem, wet_member, r, s, ctl, prog, wet_smem)) return;
+    __syncthreads();  // the item is finished by every thread; the next ticket is visible
   }
 }
 

@@ -138,6 +138,7 @@ struct BatchCtl {
   int32_t halted;      // members that raised an event during this advance call
   uint32_t ticket;     // single-launch mode: next work item, reset by every launch
   int32_t status;      // single-launch mode: nonzero if a bounded wait gave up
+  uint32_t wait_test;  // single-launch mode test hook: polls of a wait that never ends (0: off)
 };
 
 // Single-launch mode: per member, cumulative counts of finished work items
