@@ -133,7 +133,7 @@ struct Output {
       ascii(a, what, print_id);
     } else if (fmt == "BIN") {
       binary(a, what, print_id);
-    }  // GTIFF needs GDAL, which this build (like a reference build without TRITON_GDAL) does not write
+    }  // GTIFF needs GDAL: this executable, like a reference build without TRITON_GDAL, does not write it
   }
   // output_cfg (output.h:754-811): the restart cfg with four keys rewritten
   void restart_cfg(double simtime, int print_id, double average_dt, int it_count) const {
