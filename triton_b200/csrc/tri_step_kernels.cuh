@@ -304,19 +304,28 @@ __device__ __forceinline__ bool tile_skippable(const FluxCtx<T>& X, unsigned til
   return true;
 }
 
+// The same pointer, opaque to the compiler: values read through it cannot be
+// taken from an earlier read through the original.
+template <typename P>
+__device__ __forceinline__ const P* launder_ptr(const P* p) {
+  const P* q;
+  asm volatile("mov.b64 %0, %1;" : "=l"(q) : "l"(p));
+  return q;
+}
+
 // One warp tile: strip sx (30 interior columns), rows r0..r1.  kTrack:
 // record in X.tz_dst whether the tile wrote only +0 (dry-tile skipping; the
-// kernels of domains that cannot skip are built without it).
-template <typename T, bool kTrack>
-__device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, int lane) {
+// kernels of domains that cannot skip are built without it).  kReload: the
+// context (in shared memory) is read again every row instead of being held
+// in registers across the row loop; the batched kernels' member parameters
+// are not kernel parameters, and holding them spilled (FP32 batched ensemble
+// at 8 blocks per SM: 252 bytes of spill stores, 104 with the reads; 24.7
+// against 23.8 G cell-updates/s at the best launch shape).
+template <typename T, bool kTrack, bool kReload = false>
+__device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, int lane) {
+  const FluxCtx<T>& X = kReload ? *launder_ptr(&X0) : X0;
   const int rows = X.rows, cols = X.cols, rb = X.rb;
-  const T dt = X.K.dt, hextra = X.K.hextra;
-  const T* __restrict__ hi = X.hi;
-  const T* __restrict__ qxi = X.qxi;
-  const T* __restrict__ qyi = X.qyi;
-  T* __restrict__ ho = X.ho;
-  T* __restrict__ qxo = X.qxo;
-  T* __restrict__ qyo = X.qyo;
+  const T hextra = X.K.hextra;
   const int sx = (int)(tile % X.nstrips), ry = (int)(tile / X.nstrips);
   const int c = sx * kStripCols + lane;  // = c0 - 1 + lane with c0 = 1 + 30*sx
   const int r0 = 1 + ry * rb;
@@ -328,11 +337,17 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   const bool owner = incol && (mid || gcol);
   constexpr bool kAcct = true;  // FP64 volume accounts in both forms
   double acc_b = 0.0, acc_r = 0.0, acc_c = 0.0;
-  const double sxq = (double)dt / (double)X.K.dx;  // dt/dx of the boundary discharges
+  const double sxq = (double)X.K.dt / (double)X.K.dx;  // dt/dx of the boundary discharges
 
   bool wrote_nonzero = false;  // any value this lane writes is not +0
-  auto copy_ghost = [&](int r) {
-    const size_t id = (size_t)r * cols + c;
+  auto copy_ghost = [&](const FluxCtx<T>& Z, int r) {
+    const T* __restrict__ hi = Z.hi;
+    const T* __restrict__ qxi = Z.qxi;
+    const T* __restrict__ qyi = Z.qyi;
+    T* __restrict__ ho = Z.ho;
+    T* __restrict__ qxo = Z.qxo;
+    T* __restrict__ qyo = Z.qyo;
+    const size_t id = (size_t)r * Z.cols + c;
     if (kTrack) {
       const T gh = hi[id];
       ho[id] = gh;
@@ -351,40 +366,46 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
   // raw values of the next row are loaded one iteration ahead
   T lh = T(0), lqx = T(0), lqy = T(0), lz = T(0);
   double lzb = 0.0;
-  auto fetch = [&](int r) {
+  auto fetch = [&](const FluxCtx<T>& Z, int r) {
     if (incol) {
-      const size_t id = (size_t)r * cols + c;
-      lh = hi[id];
-      lqx = qxi[id];
-      lqy = qyi[id];
-      lz = X.bed.z[id];  // FP32 form: the offset from the base of the cell's tile
-      lzb = X.bed.base_at(r, c);
+      const size_t id = (size_t)r * Z.cols + c;
+      lh = Z.hi[id];
+      lqx = Z.qxi[id];
+      lqy = Z.qyi[id];
+      lz = Z.bed.z[id];  // FP32 form: the offset from the base of the cell's tile
+      lzb = Z.bed.base_at(r, c);
     }
   };
-  fetch(r0 - 1);
+  fetch(X, r0 - 1);
   CellQ<T> prev = make_cell<T>(lh, lqx, lqy, lz, hextra, lzb);
-  if (r0 - 1 == 0 && owner) copy_ghost(0);
-  fetch(r0);
+  if (r0 - 1 == 0 && owner) copy_ghost(X, 0);
+  fetch(X, r0);
   RowParts<T> pp;
   pp.r0 = pp.r1 = pp.r2 = pp.w0 = pp.w1 = pp.w2 = pp.an = T(0);
   T pn2 = T(0);  // Manning of the previous row's cell
 
   for (int r = r0; r <= r1 + 1; ++r) {
+    const FluxCtx<T>& XL = kReload ? *launder_ptr(&X0) : X0;
+    const int cols = XL.cols, rows = XL.rows;
+    const T dt = XL.K.dt, hextra = XL.K.hextra;
+    T* __restrict__ ho = XL.ho;
+    T* __restrict__ qxo = XL.qxo;
+    T* __restrict__ qyo = XL.qyo;
     const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra, lzb);
     T cn2 = T(0);
     if (r <= r1) {
-      if (upd) cn2 = X.n2[(size_t)r * cols + c];
-      fetch(r + 1);  // r1 + 1 <= rows - 1
+      if (upd) cn2 = XL.n2[(size_t)r * cols + c];
+      fetch(XL, r + 1);  // r1 + 1 <= rows - 1
     }
     FaceOut<T> Y;
     Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
-    if (upd) Y = face_flux<T, false>(cur, prev, X.K);
+    if (upd) Y = face_flux<T, false>(cur, prev, XL.K);
     if (r - 1 >= r0 && upd) {
       const size_t id = (size_t)(r - 1) * cols + c;
       T hn, qn, vn;
       double clip;
       update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn, clip,
-                     cell_hash((uint32_t)id, 2u * X.step));
+                     cell_hash((uint32_t)id, 2u * XL.step));
       if (kAcct) {
         // Inflow through the south face of a cell of the last interior row
         // (the other boundary faces are counted where their parts are
@@ -392,9 +413,9 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
         if (r - 1 == rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
         acc_c += clip;
       }
-      if (X.nroff > 0) {  // update_runoff (kernels.h:128-149)
+      if (XL.nroff > 0) {  // update_runoff (kernels.h:128-149)
         const T h0 = hn;
-        const T net = X.rates[(size_t)X.zone[id] * X.roff_rows + X.roff_row];
+        const T net = XL.rates[(size_t)XL.zone[id] * XL.roff_rows + XL.roff_row];
         if (sizeof(T) == 8) {
           hn += net * dt;
         } else if (net != T(0)) {
@@ -403,7 +424,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
           // in every cell of a binade; the FP64 sum is rounded
           // stochastically instead (unbiased), deterministic in (cell, step)
           float lo;
-          hn = sr_add(hn, net * dt, cell_hash((uint32_t)id, 2u * X.step + 1u), &lo);
+          hn = sr_add(hn, net * dt, cell_hash((uint32_t)id, 2u * XL.step + 1u), &lo);
         }
         if (hn < hextra) {
           if (hn < T(0)) hn = T(0);
@@ -418,7 +439,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
       if (kTrack) wrote_nonzero |= nonzero_bits(hn) | nonzero_bits(qn) | nonzero_bits(vn);
     }
     if (r > r1) {
-      if (r == rows - 1 && owner) copy_ghost(r);
+      if (r == rows - 1 && owner) copy_ghost(XL, r);
       break;
     }
     // x faces of row r: lane l evaluates the face between lanes l-1 and l
@@ -433,7 +454,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
     left.zb = sizeof(T) == 4 ? __shfl_up_sync(0xffffffffu, cur.zb, 1) : 0.0;
     FaceOut<T> Xf;
     Xf.a0 = Xf.a1 = Xf.a2 = Xf.b0 = Xf.b1 = Xf.b2 = T(0);
-    if (lane >= 1 && incol && c >= 1) Xf = face_flux<T, true>(left, cur, X.K);
+    if (lane >= 1 && incol && c >= 1) Xf = face_flux<T, true>(left, cur, XL.K);
     const T e0 = shfl_down1(Xf.a0), e1 = shfl_down1(Xf.a1), e2 = shfl_down1(Xf.a2);
     if (kAcct && upd) {
       // Inflow through faces shared with ghost cells, in depth units.  The
@@ -452,7 +473,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X, unsigned tile, in
     pp.w2 = Xf.b2;
     if (sizeof(T) == 4) pp.an = dev_fabs(e0) + dev_fabs(Y.a0);
     pn2 = cn2;
-    if (gcol) copy_ghost(r);
+    if (gcol) copy_ghost(XL, r);
     prev = cur;
   }
   if (kAcct) {
@@ -1200,6 +1221,7 @@ template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __restrict__ mem,
                                                           const int32_t* __restrict__ tile_member,
                                                           BatchCtl* __restrict__ ctl, uint32_t ntiles) {
+  __shared__ FluxCtx<T> s_ctx[4];  // the member context of each warp's tile
   const int lane = threadIdx.x & 31;
   while (true) {
     unsigned tile = 0;
@@ -1208,9 +1230,12 @@ __global__ void __launch_bounds__(128, MINB) k_batch_flux(const MemberDev<T>* __
     if (tile >= ntiles) break;
     const MemberDev<T>& M = mem[tile_member[tile]];
     if (!M.clk->active) continue;
-    const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
-                                     M.hextra);
-    flux_tile<T, false>(X, tile - M.tile_begin, lane);
+    __syncwarp();  // the warp's previous tile no longer reads its context
+    if (lane == 0)
+      s_ctx[threadIdx.x >> 5] = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx,
+                                            M.rdx, M.hextra);
+    __syncwarp();
+    flux_tile<T, false, true>(s_ctx[threadIdx.x >> 5], tile - M.tile_begin, lane);
   }
 }
 
@@ -1382,9 +1407,12 @@ __device__ __forceinline__ void steps_flux_item(const MemberDev<T>* __restrict__
     *seen_s = s;
   }
   if (M.clk->active) {
-    const FluxCtx<T> X = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
-                                     M.hextra);
-    flux_tile<T, false>(X, tile - M.tile_begin, lane);
+    __shared__ FluxCtx<T> s_ctx[4];  // the member context of each warp's tile, reread every row
+    if (lane == 0)
+      s_ctx[warp] = flux_ctx<T>(M.clk, M.sb, M.bed, M.n2, M.zone, M.rates, M.rows, M.cols, M.rb, M.dx, M.rdx,
+                                M.hextra);
+    __syncwarp();
+    flux_tile<T, false, true>(s_ctx[warp], tile - M.tile_begin, lane);
   }
   __syncwarp();
   if (lane == 0) {
