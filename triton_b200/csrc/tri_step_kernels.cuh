@@ -385,37 +385,37 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, i
   T pn2 = T(0);  // Manning of the previous row's cell
 
   for (int r = r0; r <= r1 + 1; ++r) {
+    // the context is read where it is used, so with kReload none of it is
+    // held across the face computations
     const FluxCtx<T>& XL = kReload ? *launder_ptr(&X0) : X0;
-    const int cols = XL.cols, rows = XL.rows;
-    const T dt = XL.K.dt, hextra = XL.K.hextra;
-    T* __restrict__ ho = XL.ho;
-    T* __restrict__ qxo = XL.qxo;
-    T* __restrict__ qyo = XL.qyo;
-    const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, hextra, lzb);
+    const CellQ<T> cur = make_cell<T>(lh, lqx, lqy, lz, XL.K.hextra, lzb);
     T cn2 = T(0);
     if (r <= r1) {
-      if (upd) cn2 = XL.n2[(size_t)r * cols + c];
+      if (upd) cn2 = XL.n2[(size_t)r * XL.cols + c];
       fetch(XL, r + 1);  // r1 + 1 <= rows - 1
     }
     FaceOut<T> Y;
     Y.a0 = Y.a1 = Y.a2 = Y.b0 = Y.b1 = Y.b2 = T(0);
     if (upd) Y = face_flux<T, false>(cur, prev, XL.K);
     if (r - 1 >= r0 && upd) {
+      const FluxCtx<T>& XU = kReload ? *launder_ptr(&X0) : X0;
+      const int cols = XU.cols;
+      const T dt = XU.K.dt, hextra = XU.K.hextra;
       const size_t id = (size_t)(r - 1) * cols + c;
       T hn, qn, vn;
       double clip;
       update_cell<T>(prev, pp, Y.b0, Y.b1, Y.b2, pn2, dt, hextra, hn, qn, vn, clip,
-                     cell_hash((uint32_t)id, 2u * XL.step));
+                     cell_hash((uint32_t)id, 2u * XU.step));
       if (kAcct) {
         // Inflow through the south face of a cell of the last interior row
         // (the other boundary faces are counted where their parts are
         // formed, below), and the depth the update clipped back to zero.
-        if (r - 1 == rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
+        if (r - 1 == XU.rows - 2) acc_b += sxq * (double)prev.qy - (double)Y.b0;
         acc_c += clip;
       }
-      if (XL.nroff > 0) {  // update_runoff (kernels.h:128-149)
+      if (XU.nroff > 0) {  // update_runoff (kernels.h:128-149)
         const T h0 = hn;
-        const T net = XL.rates[(size_t)XL.zone[id] * XL.roff_rows + XL.roff_row];
+        const T net = XU.rates[(size_t)XU.zone[id] * XU.roff_rows + XU.roff_row];
         if (sizeof(T) == 8) {
           hn += net * dt;
         } else if (net != T(0)) {
@@ -424,7 +424,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, i
           // in every cell of a binade; the FP64 sum is rounded
           // stochastically instead (unbiased), deterministic in (cell, step)
           float lo;
-          hn = sr_add(hn, net * dt, cell_hash((uint32_t)id, 2u * XL.step + 1u), &lo);
+          hn = sr_add(hn, net * dt, cell_hash((uint32_t)id, 2u * XU.step + 1u), &lo);
         }
         if (hn < hextra) {
           if (hn < T(0)) hn = T(0);
@@ -433,13 +433,16 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, i
         }
         if (kAcct) acc_r += (double)hn - (double)h0;
       }
+      T* __restrict__ ho = XU.ho;
+      T* __restrict__ qxo = XU.qxo;
+      T* __restrict__ qyo = XU.qyo;
       ho[id] = hn;
       qxo[id] = qn;
       qyo[id] = vn;
       if (kTrack) wrote_nonzero |= nonzero_bits(hn) | nonzero_bits(qn) | nonzero_bits(vn);
     }
     if (r > r1) {
-      if (r == rows - 1 && owner) copy_ghost(XL, r);
+      if (r == XL.rows - 1 && owner) copy_ghost(XL, r);
       break;
     }
     // x faces of row r: lane l evaluates the face between lanes l-1 and l
@@ -462,7 +465,7 @@ __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, i
       // boundary cell i is F(Q_i).n plus the fluctuation it receives there:
       // west / south faces dt/dx*q - b, east / north faces -(a + dt/dx*q).
       if (c == 1) acc_b += sxq * (double)cur.qx - (double)Xf.b0;
-      if (c == cols - 2) acc_b -= (double)e0 + sxq * (double)cur.qx;
+      if (c == XL.cols - 2) acc_b -= (double)e0 + sxq * (double)cur.qx;
       if (r == 1) acc_b -= (double)Y.a0 + sxq * (double)cur.qy;
     }
     pp.r0 = e0 + Y.a0;
