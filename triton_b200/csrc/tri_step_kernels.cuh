@@ -316,11 +316,13 @@ __device__ __forceinline__ const P* launder_ptr(const P* p) {
 // One warp tile: strip sx (30 interior columns), rows r0..r1.  kTrack:
 // record in X.tz_dst whether the tile wrote only +0 (dry-tile skipping; the
 // kernels of domains that cannot skip are built without it).  kReload: the
-// context (in shared memory) is read again every row instead of being held
-// in registers across the row loop; the batched kernels' member parameters
-// are not kernel parameters, and holding them spilled (FP32 batched ensemble
-// at 8 blocks per SM: 252 bytes of spill stores, 104 with the reads; 24.7
-// against 23.8 G cell-updates/s at the best launch shape).
+// context (in shared memory) is read again every row, where each value is
+// used, instead of being held in registers across the row loop; the batched
+// kernels' member parameters are not kernel parameters, and holding them
+// spilled (FP32 batched ensemble at 8 blocks per SM: 252 bytes of spill
+// stores, 20 with the reads; 25.5 against 23.8 G cell-updates/s at the best
+// launch shape).  The single-domain kernel keeps kReload off: its context
+// comes from kernel parameters, which the compiler reads at each use.
 template <typename T, bool kTrack, bool kReload = false>
 __device__ __forceinline__ void flux_tile(const FluxCtx<T>& X0, unsigned tile, int lane) {
   const FluxCtx<T>& X = kReload ? *launder_ptr(&X0) : X0;
