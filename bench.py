@@ -242,6 +242,8 @@ def workload_config(sc, desc, precision, world):
 
 def reference_arm(args, sc, desc):
     cores, logical = host_cores()
+    if args.warmup > 0 and os.path.exists(REF_EXE):
+        run_reference(sc, args.warmup, cores)  # untimed: warms the host caches and the page cache
     r = run_reference(sc, args.steps, cores)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/triton_ref_omp was not built"}))
@@ -251,11 +253,12 @@ def reference_arm(args, sc, desc):
     cfg["engine"] = (f"reference TRITON sources, OpenMP build, {cores} threads (one per physical core of "
                      f"{logical} logical CPUs)")
     line = {"metric": METRIC, "value": val, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": its,
-            "warmup": 0, "ms_per_step": 1000.0 * secs / its, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1000.0 * secs / its, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
-                             "sample": f"{its} time steps of the workload ({secs:.2f} s compute), "
-                                       f"{cores} OpenMP threads on {cores} physical cores"},
+                             "sample": f"{its} time steps of the workload ({secs:.2f} s compute) after an "
+                                       f"untimed run of {args.warmup}, {cores} OpenMP threads on {cores} "
+                                       f"physical cores"},
             "e2e": {"value": val, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
